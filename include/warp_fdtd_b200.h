@@ -1,0 +1,210 @@
+/*
+ * warp_fdtd_b200 — C ABI of the B200 (sm_100a) uniform-grid FDTD library.
+ *
+ * Every entry point takes raw device pointers, sizes and a cudaStream_t passed
+ * as void* (NULL = legacy default stream), launches asynchronously on that
+ * stream and returns FDTD_OK (0) or a negative status; nothing is allocated or
+ * freed and no ownership is transferred.  fdtd_last_error() returns a message
+ * for the last failure on the calling thread.
+ *
+ * Layout (warp_fdtd/kernels.py:25): a field is (3, n) float32, n = nx*ny*nz,
+ * flat index i = (x*ny + y)*nz + z with z fastest.  A 2-D argument is passed
+ * with its column count ("*_cols") so that arrays of other widths (such as the
+ * reference tests' (3, 1) placeholders) are addressed as the reference does.
+ *
+ * Two groups of entry points:
+ *  1. Kernel-level replacements of the reference's Warp kernels, same
+ *     arguments in the same order and the same in-place semantics.  Each cites
+ *     the kernel it replaces.
+ *  2. The B200 forward path the Solver uses: one fused E+H step over
+ *     ping-pong buffers plus float64 multi-frequency detector recorders.
+ */
+#ifndef WARP_FDTD_B200_H
+#define WARP_FDTD_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDTD_OK 0
+#define FDTD_ERR_ARG (-1)   /* invalid size, pointer or option */
+#define FDTD_ERR_CUDA (-2)  /* a CUDA launch or runtime call failed */
+
+/* Message for the last non-zero status returned on this thread. */
+const char *fdtd_last_error(void);
+
+/* Library ABI version (major*100 + minor). */
+int fdtd_version(void);
+
+/* ---------------------------------------------------------------------------
+ * 1. Kernel-level replacements
+ * ------------------------------------------------------------------------ */
+
+/* Replaces kernels.py:77-148 update_e / update_h / update_e_packed /
+ * update_h_packed (`make_update(electric, packed)`), launched over n cells.
+ * f (3, fg_cols) is updated in place from g; psi (6, psi_cols) holds f's CPML
+ * state; coeff is (3, clen, 3) float (a, b, 1/kappa) or, with packed != 0,
+ * (3, clen, 4) with the plane rank of solver.py:16-29 pack_coefficients;
+ * source (3, source_cols) and waves (3, waves_cols) inject the plane source
+ * at x == source_x (source_x < 0 disables it); step is the device step
+ * counter; when electric == 0 and step >= save_h_from the old H is copied to
+ * hprev (3, hprev_cols).  periodic != 0 wraps neighbours (kernels.py:19-22). */
+int fdtd_update(int electric, int packed, float *f, const float *g, long long fg_cols,
+                const float *inv_eps, float *psi, long long psi_cols, const float *coeff,
+                int clen, const float *source, long long source_cols, const float *waves,
+                long long waves_cols, const int *step, float *hprev, long long hprev_cols,
+                int save_h_from, int nx, int ny, int nz, int source_x, float courant,
+                int periodic, void *stream);
+
+/* Replaces kernels.py:151-153 `advance` (delta = +1) and adjoint.py:226-228
+ * `retreat` (delta = -1): step[0] += delta on the device. */
+int fdtd_advance(int *step, int delta, void *stream);
+
+/* Replaces detectors.py:65-106 `record`, launched over count = sx*sy*sz
+ * plane cells starting at (x0, y0, z0).  weights is (steps, 2) float32
+ * (complex64 as re, im), indices (steps) int32, phasor (6, count, 2) float32,
+ * flux (bins) float32, area (count) float32.  Fields e, h, prev are (3, cols).
+ * Phasor cells accumulate exactly as the reference (float32); flux bins are
+ * added with float32 atomics, as the reference does. */
+int fdtd_record(const float *e, const float *h, const float *prev, long long cols,
+                const int *step, const float *weights, const int *indices, float *phasor,
+                float *flux, const float *area, int nx, int ny, int nz, int x0, int y0,
+                int z0, int sx, int sy, int sz, int axis, int exact, int is_phasor,
+                void *stream);
+
+/* Replaces adjoint.py:17-43 `record_curl`: hist[step, c, j] = courant *
+ * curl(H)_c over the design box (x0, y0, z0, sx, sy, sz); hist is
+ * (steps, 3, sx*sy*sz). */
+int fdtd_record_curl(const float *h, long long cols, float *hist, const int *step, int nx,
+                     int ny, int nz, int x0, int y0, int z0, int sx, int sy, int sz,
+                     float courant, void *stream);
+
+/* Replaces adjoint.py:46-88 `prepare` (transpose of the field scaling and the
+ * CPML recurrence).  q (3, n), eps (n), psi (6, n), coeff (3, clen, 3),
+ * d (6, n). */
+int fdtd_prepare(const float *q, const float *eps, float *psi, const float *coeff, int clen,
+                 float *d, int nx, int ny, int nz, float courant, int electric,
+                 void *stream);
+
+/* Replaces adjoint.py:107-162 `gather` (q += D^T d; with from_h, the design
+ * inner product grad[j] += sum_c hist[step, c, j] * q_c).  grad is float32
+ * (grad_f64 == 0, as the reference) or float64 (grad_f64 != 0). */
+int fdtd_gather(float *q, const float *d, const float *hist, void *grad, int grad_f64,
+                const int *step, int nx, int ny, int nz, int x0, int y0, int z0, int sx,
+                int sy, int sz, int from_h, void *stream);
+
+/* Replaces adjoint.py:181-223 `inject` (transpose of detector colocation):
+ * source (6, count, 2) float32, weights (steps, 2); scattered with float32
+ * atomics as the reference does. */
+int fdtd_inject(float *qe, float *qh, const float *source, const float *weights,
+                const int *step, int nx, int ny, int nz, int x0, int y0, int z0, int sx,
+                int sy, int sz, int old_h_only, void *stream);
+
+/* Replaces adjoint.py:472-490 `write_design`: eps[box] = plane[x, y] for all z
+ * in the box; plane is (sx, sy) float32. */
+int fdtd_write_design(const float *plane, float *eps, int nx, int ny, int nz, int x0,
+                      int y0, int z0, int sx, int sy, int sz, void *stream);
+
+/* Replaces material.py:12-25 `smooth`: out = clamp-extended 2-D correlation
+ * of p (px, py) with weights (2r+1, 2r+1), r = radius (the reference uses 9). */
+int fdtd_material_smooth(const float *p, const float *weights, int radius, float *out,
+                         int px, int py, void *stream);
+
+/* Replaces material.py:35-55 `subpixel` (+ `project` 28-32): out =
+ * 1 / (eps_lo + contrast * projected(rho)); the reference's map has
+ * eps_lo = 1 and contrast = 11.25. */
+int fdtd_material_subpixel(const float *rho, float *out, int px, int py, float beta,
+                           float eps_lo, float contrast, void *stream);
+
+/* Reverse mode of fdtd_material_subpixel (the reference differentiates it with
+ * a Warp Tape, material.py:93-102): rho_grad += d out/d rho ^T g. */
+int fdtd_material_subpixel_adjoint(const float *rho, const float *g, float *rho_grad,
+                                   int px, int py, float beta, float eps_lo,
+                                   float contrast, void *stream);
+
+/* Reverse mode of fdtd_material_smooth: p_grad += smooth^T g (clamp edges fold
+ * their weight back onto the edge pixel). */
+int fdtd_material_smooth_adjoint(const float *g, const float *weights, int radius,
+                                 float *p_grad, int px, int py, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * 2. B200 forward path
+ * ------------------------------------------------------------------------ */
+
+/* Arguments of one fused leapfrog step (E then H), the work of
+ * solver.py:194-237's update_e + update_h launches.  Buffers ping-pong: with
+ * t = step[0] and s = t & 1 the step reads E[s], H[s], psi_*[s] and writes
+ * E[s^1], H[s^1], psi_*[s^1], so after the step H[s] still holds H(n-1/2)
+ * (the reference's hprev).  It does not advance step[0].
+ *
+ * Rows may be padded: cell (x, y, z) of a field, of full-storage psi and of
+ * inv_eps lives at (x*ny + y)*pitch_z + z, and of the uint8 material at
+ * (x*ny + y)*material_pitch + z.  Padding cells must hold zeros (fields) and
+ * are never written.  The TMA pipeline (path 2) needs pitch_z % 4 == 0,
+ * material_pitch % 16 == 0 and 16-byte aligned buffers; path 0 picks it
+ * whenever those hold and falls back to the shared-memory path (1). */
+typedef struct fdtd_step_args {
+    float *E[2];
+    float *H[2];
+    float *psi_e[2];           /* (6, psi_cols) each */
+    float *psi_h[2];
+    long long psi_cols;        /* nx*ny*pitch_z (full storage) or packed slab size */
+    const float *coeff_e;      /* (3, clen, 4): a, b, 1/kappa, packed plane rank */
+    const float *coeff_h;
+    int clen;
+    int packed;                /* 0: psi indexed by cell, 1: by packed plane rank */
+    int material_kind;         /* 0: inv_eps per cell, 1: uint8 index into table */
+    const float *inv_eps;      /* per cell float32, material_kind 0 */
+    const uint8_t *material;   /* per cell uint8, material_kind 1 */
+    const float *material_table; /* (material_count) inverse permittivities */
+    int material_count;        /* <= 256 */
+    const float *src_e;        /* (3, ny*nz) E profile (drives the H update) */
+    const float *src_h;        /* (3, ny*nz) H profile (drives the E update) */
+    const float *waves_e;      /* (3, waves_cols) */
+    const float *waves_h;
+    long long waves_cols;      /* steps with t >= waves_cols inject nothing */
+    int source_x;              /* < 0: no source */
+    float courant;
+    const int *step;
+    int nx, ny, nz;
+    int pitch_z;               /* 0: nz */
+    int material_pitch;        /* 0: nz */
+    int tile_y, tile_z, chunk_x; /* launch shape; 0 picks defaults */
+    int path;                  /* 0 auto, 1 shared-memory staging, 2 TMA pipeline */
+    int *error;                /* optional device int, set to 1 if a bounded wait expires */
+} fdtd_step_args;
+
+int fdtd_step_fused(const fdtd_step_args *args, void *stream);
+
+/* Float64 running DFT at one detector plane for K frequencies (the phasor
+ * branch of detectors.py:65-106 generalised), run after fdtd_step_fused and
+ * before the step counter advances.  With t = step[0] and s = t & 1 the new
+ * fields are E[s^1], H[s^1] and H(n-1/2) is H[s] (the reference's hprev); the
+ * field rows have pitch `pitch_z`.  If t < nsteps and indices[t] >= 0,
+ * phasor[k, c, i] (re, im) += w[k, t] * f_c for the six colocated
+ * (exact != 0) or raw components f_c, the fp32 sample and weight promoted to
+ * float64.  indices (nsteps) int32; weights (K, nsteps, 2) float32; phasor
+ * (K, 6, count, 2) float64. */
+int fdtd_record_phasor64(const float *E0, const float *E1, const float *H0, const float *H1,
+                         const int *step, const int *indices, int nsteps,
+                         const float *weights, int nfreq, double *phasor, int nx, int ny,
+                         int nz, int pitch_z, int x0, int y0, int z0, int sx, int sy, int sz,
+                         int exact, void *stream);
+
+/* Flux branch of detectors.py:104-106 with float64 bins, same buffer
+ * convention as fdtd_record_phasor64: if t < nsteps and 0 <= indices[t] <
+ * nbins, flux[indices[t]] += sum over the plane of cross(E, H)[axis] * area
+ * (fp32 products summed in float64). */
+int fdtd_record_flux64(const float *E0, const float *E1, const float *H0, const float *H1,
+                       const int *step, const int *indices, int nsteps, const float *area,
+                       double *flux, int nbins, int nx, int ny, int nz, int pitch_z, int x0,
+                       int y0, int z0, int sx, int sy, int sz, int axis, int exact,
+                       void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WARP_FDTD_B200_H */

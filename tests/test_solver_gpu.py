@@ -1,0 +1,177 @@
+"""Solver-level parity on the reference's own bundles.
+
+* forward50_gpu (80x80x30, 2098 steps, two raw flux detectors): the port of
+  the reference's tests/test_warp_solver.py, plus bitwise equality with the
+  CPU oracle and field rel-L2 against the reference's Warp float32 output.
+* hann_200fs (200x200x75, 5245 steps, colocated flux + three mode
+  detectors): mid-z fields, mode phasors and modal transmission against the
+  Warp outputs the reference committed (results/warp/hann20)."""
+
+import json
+import sys
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+from conftest import GOLDEN  # noqa: E402
+
+FIELD_TOL = 1e-5      # field rel-L2 vs the reference's Warp float32 path
+MODAL_T_TOL = 1e-5    # |T - T_warp| absolute
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    dt = np.complex128 if (np.iscomplexobj(a) or np.iscomplexobj(b)) else np.float64
+    a, b = a.astype(dt), b.astype(dt)
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+@pytest.fixture(scope="module")
+def s50():
+    from warp_fdtd_b200.solver import Solver
+    from warp_fdtd_b200.detectors import attach
+
+    s = Solver(GOLDEN / "forward50_gpu", graph_steps=64)
+    attach(s)
+    s.compile()
+    return s
+
+
+@pytest.fixture(scope="module")
+def oracle50():
+    from oracle.model import OracleSolver
+
+    o = OracleSolver(GOLDEN / "forward50_gpu").attach()
+    o.run()
+    return o
+
+
+def test_source_staggering(s50):
+    """tests/test_warp_solver.py:18-25: after one step E == 0 exactly, H is not."""
+    s50.reset()
+    s50.launch_step()
+    torch.cuda.synchronize()
+    assert float(s50.E.abs().max()) == 0
+    assert float(s50.H.abs().max()) > 1e-5
+
+
+def test_full_3d_fields_flux_and_reset(s50):
+    """tests/test_warp_solver.py:27-48 with the Warp golden as reference."""
+    s = s50
+    s.reset()
+    s.run()
+    a = s.fields()
+    assert int(s.step.cpu()[0]) == s.steps
+    warp = np.load(GOLDEN / "forward50_gpu" / "warp_fields.npz")
+    fdtdx = np.load(GOLDEN / "forward50_gpu" / "fdtdx_flux.npz")
+    for name in ("E", "H"):
+        assert np.isfinite(a[name]).all()
+        assert rel(a[name], warp[name]) < FIELD_TOL, (name, rel(a[name], warp[name]))
+    for m in s.monitors:
+        b = m.flux.cpu().numpy()
+        assert rel(b, fdtdx[m.name].ravel()) < 1e-3
+    s.reset()
+    s.run()
+    b = s.fields()
+    for name in ("E", "H"):
+        np.testing.assert_array_equal(a[name], b[name])
+    assert "jax" not in sys.modules and "warp" not in sys.modules
+
+
+def test_forward50_bitwise_equal_to_oracle(s50, oracle50):
+    s50.reset()
+    s50.run()
+    a = s50.fields()
+    o = oracle50.fields()
+    np.testing.assert_array_equal(a["E"], o["E"])
+    np.testing.assert_array_equal(a["H"], o["H"])
+    for m, om in zip(s50.monitors, oracle50.monitors):
+        got = m.flux.cpu().numpy()
+        np.testing.assert_allclose(got, om.flux, rtol=1e-12, atol=1e-30)
+
+
+def test_packed_storage_and_eager_path_identical(s50):
+    from warp_fdtd_b200.solver import Solver, owned_array_bytes
+    from warp_fdtd_b200.detectors import attach
+
+    s50.reset()
+    s50.run()
+    ref = s50.fields()
+    p = Solver(GOLDEN / "forward50_gpu", cpml_storage="packed", graph_steps=100)
+    attach(p)
+    p.compile()
+    p.run()
+    for name, arr in p.fields().items():
+        np.testing.assert_array_equal(arr, ref[name])
+    assert p._psi_cols < s50.n
+    assert owned_array_bytes(p) < owned_array_bytes(s50)
+    # no graphs: one eager launch per step
+    q = Solver(GOLDEN / "forward50_gpu")
+    attach(q)
+    q.reset()
+    q.run()
+    for name, arr in q.fields().items():
+        np.testing.assert_array_equal(arr, ref[name])
+
+
+def test_tile_shapes_identical(s50):
+    s50.reset()
+    s50.run()
+    ref = s50.fields()
+    from warp_fdtd_b200.solver import Solver
+
+    for tile, path in [((4, 16, 7), 2), ((16, 32, 80), 2), ((8, 64, 3), 2), ((0, 0, 0), 1),
+                       ((4, 8, 9), 1)]:
+        s = Solver(GOLDEN / "forward50_gpu", tile=tile, path=path)
+        s.reset()
+        s.run()
+        for name, arr in s.fields().items():
+            np.testing.assert_array_equal(arr, ref[name])
+
+
+@pytest.fixture(scope="module")
+def s200():
+    from warp_fdtd_b200.solver import Solver
+    from warp_fdtd_b200.detectors import attach
+
+    s = Solver(GOLDEN / "hann_200fs")
+    attach(s)
+    s.compile()
+    s.reset()
+    s.run()
+    return s
+
+
+def test_hann20_fields_vs_warp(s200):
+    warp = np.load(GOLDEN / "hann_200fs" / "warp_fields.npz")
+    f = s200.fields()
+    for name in ("E", "H"):
+        a = f[name][..., f[name].shape[-1] // 2]
+        assert rel(a, warp[name]) < FIELD_TOL, (name, rel(a, warp[name]))
+
+
+def test_hann20_mode_phasors_and_transmission_vs_warp(s200):
+    from warp_fdtd_b200.detectors import measurements
+
+    mons = {m.name: m for m in s200.monitors}
+    for name in ("mode_in", "mode_out"):
+        want = np.load(GOLDEN / "hann_200fs" / f"warp_{name}_phasors.npz")["phasors"]
+        got = mons[name].phasors()
+        assert rel(got, want) < FIELD_TOL, (name, rel(got, want))
+    meas = measurements(s200)
+    ref = json.loads((GOLDEN / "hann_200fs" / "warp_result.json").read_text())["measurements"]
+    assert abs(meas["modal_transmission"] - ref["modal_transmission"]) < MODAL_T_TOL
+    assert abs(meas["modal_reflection"] - ref["modal_reflection"]) < MODAL_T_TOL
+    for key in ("mode_in", "mode_out"):
+        assert abs(meas[key] - ref[key]) / ref[key] < 1e-5
+
+
+def test_hann20_flux_vs_fdtdx(s200):
+    fdtdx = np.load(GOLDEN / "hann_200fs" / "fdtdx_flux.npz")
+    for m in s200.monitors:
+        if m.is_phasor:
+            continue
+        assert rel(m.flux.cpu().numpy(), fdtdx[m.name].ravel()) < 1e-3

@@ -1,0 +1,142 @@
+"""ctypes binding of libwarp_fdtd_b200.so (the C ABI in include/warp_fdtd_b200.h).
+
+The library is the only compute path: if it is missing or fails to load, every
+entry point raises; nothing falls back to the CPU.
+"""
+
+import ctypes
+from pathlib import Path
+
+import torch
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libwarp_fdtd_b200.so"
+
+FDTD_OK = 0
+FDTD_ERR_ARG = -1
+FDTD_ERR_CUDA = -2
+
+_p = ctypes.c_void_p
+_i = ctypes.c_int
+_ll = ctypes.c_longlong
+_f = ctypes.c_float
+
+
+class StepArgs(ctypes.Structure):
+    """Mirror of `fdtd_step_args`."""
+
+    _fields_ = [
+        ("E", _p * 2),
+        ("H", _p * 2),
+        ("psi_e", _p * 2),
+        ("psi_h", _p * 2),
+        ("psi_cols", _ll),
+        ("coeff_e", _p),
+        ("coeff_h", _p),
+        ("clen", _i),
+        ("packed", _i),
+        ("material_kind", _i),
+        ("inv_eps", _p),
+        ("material", _p),
+        ("material_table", _p),
+        ("material_count", _i),
+        ("src_e", _p),
+        ("src_h", _p),
+        ("waves_e", _p),
+        ("waves_h", _p),
+        ("waves_cols", _ll),
+        ("source_x", _i),
+        ("courant", _f),
+        ("step", _p),
+        ("nx", _i),
+        ("ny", _i),
+        ("nz", _i),
+        ("pitch_z", _i),
+        ("material_pitch", _i),
+        ("tile_y", _i),
+        ("tile_z", _i),
+        ("chunk_x", _i),
+        ("path", _i),
+        ("error", _p),
+    ]
+
+
+# name -> argtypes (all return int status)
+_SIGNATURES = {
+    "fdtd_update": [_i, _i, _p, _p, _ll, _p, _p, _ll, _p, _i, _p, _ll, _p, _ll, _p, _p, _ll,
+                    _i, _i, _i, _i, _i, _f, _i, _p],
+    "fdtd_advance": [_p, _i, _p],
+    "fdtd_record": [_p, _p, _p, _ll, _p, _p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i,
+                    _i, _i, _i, _i, _p],
+    "fdtd_record_curl": [_p, _ll, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i, _f, _p],
+    "fdtd_prepare": [_p, _p, _p, _p, _i, _p, _i, _i, _i, _f, _i, _p],
+    "fdtd_gather": [_p, _p, _p, _p, _i, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i, _i, _p],
+    "fdtd_inject": [_p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i, _i, _p],
+    "fdtd_write_design": [_p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i, _p],
+    "fdtd_material_smooth": [_p, _p, _i, _p, _i, _i, _p],
+    "fdtd_material_smooth_adjoint": [_p, _p, _i, _p, _i, _i, _p],
+    "fdtd_material_subpixel": [_p, _p, _i, _i, _f, _f, _f, _p],
+    "fdtd_material_subpixel_adjoint": [_p, _p, _p, _i, _i, _f, _f, _f, _p],
+    "fdtd_step_fused": [ctypes.POINTER(StepArgs), _p],
+    "fdtd_record_phasor64": [_p, _p, _p, _p, _p, _p, _i, _p, _i, _p, _i, _i, _i, _i, _i, _i,
+                             _i, _i, _i, _i, _i, _p],
+    "fdtd_record_flux64": [_p, _p, _p, _p, _p, _p, _i, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i,
+                           _i, _i, _i, _i, _i, _p],
+}
+
+EXPORTS = sorted(_SIGNATURES) + ["fdtd_last_error", "fdtd_version"]
+
+_lib = None
+
+
+class FdtdError(RuntimeError):
+    pass
+
+
+def load():
+    """Load the library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise FdtdError(
+                f"{LIB_PATH.name} is not built; run `python -m warp_fdtd_b200.build`"
+            )
+        lib = ctypes.CDLL(str(LIB_PATH))
+        for name, argtypes in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = argtypes
+            fn.restype = _i
+        lib.fdtd_last_error.restype = ctypes.c_char_p
+        lib.fdtd_last_error.argtypes = []
+        lib.fdtd_version.restype = _i
+        _lib = lib
+    return _lib
+
+
+def call(name, *args):
+    """Call an entry point and raise on a non-zero status."""
+    lib = load()
+    status = getattr(lib, name)(*args)
+    if status != FDTD_OK:
+        msg = lib.fdtd_last_error().decode(errors="replace")
+        if status == FDTD_ERR_ARG:
+            raise ValueError(msg)
+        raise FdtdError(msg)
+    return status
+
+
+def ptr(t):
+    """Device pointer of a tensor (None -> NULL)."""
+    if t is None:
+        return None
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"expected a torch.Tensor, got {type(t).__name__}")
+    if t.device.type != "cuda":
+        raise ValueError("warp_fdtd_b200 kernels take CUDA tensors only")
+    if not t.is_contiguous():
+        raise ValueError("warp_fdtd_b200 kernels take contiguous tensors only")
+    return t.data_ptr()
+
+
+def stream_handle(device=None):
+    return torch.cuda.current_stream(device).cuda_stream

@@ -1,0 +1,137 @@
+// Float64 detector recorders for the fused forward path (detectors.py:65-106
+// generalised to K DFT frequencies).  They run after fdtd_step_fused on the
+// same stream and pick the ping-pong buffers by the step parity, so a CUDA
+// graph of steps replays them unchanged.
+#include "common.cuh"
+
+namespace wfb {
+
+__global__ void record_phasor64_kernel(const float *__restrict__ E0, const float *__restrict__ E1,
+                                       const float *__restrict__ H0, const float *__restrict__ H1,
+                                       const int *__restrict__ step,
+                                       const int *__restrict__ indices, int nsteps,
+                                       const float2 *__restrict__ weights, int nfreq,
+                                       double2 *__restrict__ phasor, int nx, int ny, int nz,
+                                       int pitch, int x0, int y0, int z0, int sx, int sy, int sz,
+                                       int exact) {
+    const i64 count = (i64)sx * sy * sz;
+    i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int t = step[0];
+    if (t < 0 || t >= nsteps || indices[t] < 0) return;
+    const i64 wsteps = nsteps;
+    const int s = t & 1;
+    const float *e = s ? E0 : E1;
+    const float *h = s ? H0 : H1;
+    const float *prev = s ? H1 : H0;
+    const i64 n = (i64)nx * ny * pitch;
+    int x = x0 + (int)(i / ((i64)sy * sz));
+    int y = y0 + (int)((i / sz) % sy);
+    int z = z0 + (int)(i % sz);
+    float ee[3], hh[3];
+    plane_sample(e, h, prev, n, x, y, z, nx, ny, nz, exact, ee, hh, pitch);
+    for (int k = 0; k < nfreq; ++k) {
+        float2 w = weights[(i64)k * wsteps + t];
+        double wr = w.x, wi = w.y;
+        if (wr == 0.0 && wi == 0.0) continue;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) {
+            double v = c < 3 ? (double)ee[c] : (double)hh[c - 3];
+            double2 *p = phasor + ((i64)k * 6 + c) * count + i;
+            double2 acc = *p;
+            acc.x = acc.x + wr * v;
+            acc.y = acc.y + wi * v;
+            *p = acc;
+        }
+    }
+}
+
+__global__ void record_flux64_kernel(const float *__restrict__ E0, const float *__restrict__ E1,
+                                     const float *__restrict__ H0, const float *__restrict__ H1,
+                                     const int *__restrict__ step,
+                                     const int *__restrict__ indices, int nsteps,
+                                     const float *__restrict__ area, double *__restrict__ flux,
+                                     int nbins, int nx, int ny, int nz, int pitch, int x0,
+                                     int y0, int z0, int sx, int sy, int sz, int axis,
+                                     int exact) {
+    __shared__ double partial[32];
+    const i64 count = (i64)sx * sy * sz;
+    const int t = step[0];
+    if (t < 0 || t >= nsteps) return;
+    const int index = indices[t];
+    if (index < 0 || index >= nbins) return;
+    const int s = t & 1;
+    const float *e = s ? E0 : E1;
+    const float *h = s ? H0 : H1;
+    const float *prev = s ? H1 : H0;
+    const i64 n = (i64)nx * ny * pitch;
+    double acc = 0.0;
+    for (i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (i64)gridDim.x * blockDim.x) {
+        int x = x0 + (int)(i / ((i64)sy * sz));
+        int y = y0 + (int)((i / sz) % sy);
+        int z = z0 + (int)(i % sz);
+        float ee[3], hh[3];
+        plane_sample(e, h, prev, n, x, y, z, nx, ny, nz, exact, ee, hh, pitch);
+        float power = cross_axis(ee, hh, axis) * area[i];
+        acc += (double)power;
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) partial[warp] = acc;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+        acc = lane < nw ? partial[lane] : 0.0;
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if (lane == 0) atomicAdd(flux + index, acc);
+    }
+}
+
+}  // namespace wfb
+
+using namespace wfb;
+
+extern "C" {
+
+int fdtd_record_phasor64(const float *E0, const float *E1, const float *H0, const float *H1,
+                         const int *step, const int *indices, int nsteps,
+                         const float *weights, int nfreq, double *phasor, int nx, int ny,
+                         int nz, int pitch_z, int x0, int y0, int z0, int sx, int sy, int sz,
+                         int exact, void *stream) {
+    const i64 count = (i64)sx * sy * sz;
+    if (pitch_z <= 0) pitch_z = nz;
+    if (count <= 0 || nfreq < 1 || nsteps < 1 || pitch_z < nz || !E0 || !E1 || !H0 || !H1 ||
+        !step || !indices || !weights || !phasor || x0 < 0 || y0 < 0 || z0 < 0 ||
+        x0 + sx > nx || y0 + sy > ny || z0 + sz > nz) {
+        set_error("fdtd_record_phasor64: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    record_phasor64_kernel<<<(unsigned)((count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        E0, E1, H0, H1, step, indices, nsteps, (const float2 *)weights, nfreq,
+        (double2 *)phasor, nx, ny, nz, pitch_z, x0, y0, z0, sx, sy, sz, exact);
+    return launch_status("fdtd_record_phasor64");
+}
+
+int fdtd_record_flux64(const float *E0, const float *E1, const float *H0, const float *H1,
+                       const int *step, const int *indices, int nsteps, const float *area,
+                       double *flux, int nbins, int nx, int ny, int nz, int pitch_z, int x0,
+                       int y0, int z0, int sx, int sy, int sz, int axis, int exact,
+                       void *stream) {
+    const i64 count = (i64)sx * sy * sz;
+    if (pitch_z <= 0) pitch_z = nz;
+    if (count <= 0 || axis < 0 || axis > 2 || nsteps < 1 || nbins < 1 || pitch_z < nz ||
+        !E0 || !E1 || !H0 || !H1 || !step || !indices || !area || !flux || x0 < 0 || y0 < 0 ||
+        z0 < 0 || x0 + sx > nx || y0 + sy > ny || z0 + sz > nz) {
+        set_error("fdtd_record_flux64: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    i64 blocks = (count + 255) / 256;
+    if (blocks > 148) blocks = 148;
+    record_flux64_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(
+        E0, E1, H0, H1, step, indices, nsteps, area, flux, nbins, nx, ny, nz, pitch_z, x0, y0,
+        z0, sx, sy, sz, axis, exact);
+    return launch_status("fdtd_record_flux64");
+}
+
+}  // extern "C"

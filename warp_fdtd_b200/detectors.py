@@ -1,0 +1,185 @@
+"""Drop-in for warp_fdtd/detectors.py: colocated phasor and flux detectors.
+
+`Monitor`, `attach` and `measurements` keep the reference's names, arguments
+and results (detectors.py:109-232).  Differences, all in accuracy's favour:
+
+* phasors accumulate in float64 (K frequencies at once; the reference keeps
+  one complex64 phasor at the source frequency);
+* flux bins are float64 plane sums instead of float32 atomics;
+* monitors that sample the same plane with the same weights (the reference
+  bundles' mode_in and mode_reflected) share one accumulator.
+
+The kernel-level `record` (detectors.py:65-106) with the reference's float32
+semantics is exported as a launchable for code that drives kernels directly.
+"""
+
+import numpy as np
+import torch
+
+from . import _lib
+from .kernels import Kernel
+from ._lib import ptr
+
+
+def _record(e, h, prev, step, weights, indices, phasor, flux, area, nx, ny, nz, x0, y0, z0,
+            sy, sz, axis, exact, is_phasor, count=None, stream=None):
+    """detectors.py:65-106; launch size count = sx*sy*sz (sx inferred from area)."""
+    count = int(area.numel()) if count is None else int(count)
+    sx = count // (int(sy) * int(sz))
+    _lib.call(
+        "fdtd_record", ptr(e), ptr(h), ptr(prev), int(e.shape[1]), ptr(step), ptr(weights),
+        ptr(indices), ptr(phasor), ptr(flux), ptr(area), int(nx), int(ny), int(nz), int(x0),
+        int(y0), int(z0), sx, int(sy), int(sz), int(axis), int(exact), int(is_phasor),
+        stream if stream is not None else _lib.stream_handle(),
+    )
+
+
+record = Kernel("record", _record, lambda *a: int(a[8].numel()))
+
+
+class Monitor:
+    def __init__(self, solver, obj):
+        self.obj = obj
+        self.name = obj["name"]
+        self.is_phasor = obj["class"] in ("ModeOverlapDetector", "PhasorDetector")
+        if obj["class"] not in ("ModeOverlapDetector", "PhasorDetector", "PoyntingFluxDetector"):
+            raise ValueError(f"Unsupported detector {obj['class']}")
+        self.shape = tuple(hi - lo for lo, hi in obj["grid_slice"])
+        self.n = int(np.prod(self.shape))
+        self.lo = [a for a, b in obj["grid_slice"]]
+        nx, ny, nz = solver.shape
+        for a, (lo, hi) in enumerate(obj["grid_slice"]):
+            if not 0 <= lo < hi <= solver.shape[a]:
+                raise ValueError(f"Detector {self.name} lies outside the grid")
+        self.exact = bool(
+            self.is_phasor or solver.meta["settings"].get("exact_interpolation", False)
+        )
+        indices = np.ascontiguousarray(solver.data[self.name + "/_time_step_to_arr_idx"], np.int32)
+        if indices.shape != (solver.steps,):
+            raise ValueError(f"Detector {self.name} schedule must have one entry per step")
+        dev = solver.device
+        self.indices = torch.from_numpy(indices).to(dev)
+        self.first = int(np.flatnonzero(indices >= 0)[0])
+        src = next(o for o in solver.meta["objects"] if o["class"] == "ModePlaneSource")
+        self.frequencies = [float(f) for f in obj.get("frequencies_hz", [src["frequency_hz"]])]
+        K = len(self.frequencies)
+        weights = np.zeros((K, solver.steps), np.complex64)
+        if self.is_phasor:
+            # detectors.py:133-141, per frequency
+            t = np.arange(solver.steps, dtype=np.float32) * np.float32(solver.meta["dt_s"])
+            window = solver.data[self.name + "/_window_at_time_step_arr"]
+            for j, f in enumerate(self.frequencies):
+                phase = np.float32(2 * np.pi * f) * t
+                weights[j] = (
+                    np.exp(1j * phase).astype(np.complex64)
+                    * np.float32(2 / obj["window_sum"])
+                    * window
+                )
+        self.weights_numpy = weights
+        self.weights = torch.from_numpy(
+            np.ascontiguousarray(np.stack((weights.real, weights.imag), axis=-1), np.float32)
+        ).to(dev)
+        self.phasor = torch.zeros((K, 6, self.n if self.is_phasor else 1, 2),
+                                  dtype=torch.float64, device=dev)
+        self.flux = torch.zeros(int(indices.max()) + 1, dtype=torch.float64, device=dev)
+        self.axis = obj.get("propagation_axis", 2)
+        widths = []
+        for a, axis in enumerate("xyz"):
+            lo, hi = obj["grid_slice"][a]
+            v = (
+                np.diff(solver.data[axis + "_edges_m"])[lo:hi]
+                if a != self.axis
+                else np.ones(hi - lo, np.float32)
+            )
+            sh = [1, 1, 1]
+            sh[a] = len(v)
+            widths.append(v.reshape(sh))
+        self.area_numpy = np.broadcast_to(widths[0] * widths[1] * widths[2], self.shape).copy()
+        if obj["class"] == "ModeOverlapDetector":
+            self.area_numpy /= self.area_numpy.mean()
+        self.area = torch.from_numpy(
+            np.ascontiguousarray(self.area_numpy.ravel(), np.float32)).to(dev)
+        self.shared = None  # monitor whose accumulator this one aliases
+
+    def _key(self):
+        return (tuple(map(tuple, self.obj["grid_slice"])), self.exact, self.is_phasor,
+                self.weights_numpy.tobytes(), self.indices.cpu().numpy().tobytes())
+
+    def reset(self):
+        if self.shared is None:
+            self.phasor.zero_()
+            self.flux.zero_()
+
+    def launch(self, s):
+        if self.shared is not None:
+            return
+        nx, ny, nz = s.shape
+        stream = _lib.stream_handle(s.device)
+        common = (ptr(s._E[0]), ptr(s._E[1]), ptr(s._H[0]), ptr(s._H[1]), ptr(s.step))
+        steps = int(self.indices.numel())
+        if self.is_phasor:
+            _lib.call(
+                "fdtd_record_phasor64", *common, ptr(self.indices), steps, ptr(self.weights),
+                int(self.weights.shape[0]), ptr(self.phasor), nx, ny, nz, s._pitch, *self.lo,
+                *self.shape, int(self.exact), stream,
+            )
+        else:
+            _lib.call(
+                "fdtd_record_flux64", *common, ptr(self.indices), steps, ptr(self.area),
+                ptr(self.flux), int(self.flux.numel()), nx, ny, nz, s._pitch, *self.lo,
+                *self.shape, int(self.axis), int(self.exact), stream,
+            )
+
+    def phasors(self, k=0):
+        raw = self.phasor[k].cpu().numpy()
+        return (raw[..., 0] + 1j * raw[..., 1]).reshape(6, *self.shape)
+
+    def power(self, s, k=0):
+        """detectors.py:203-211 (complex128 overlap on the host)."""
+        ph = self.phasors(k)
+        me = s.data[self.name + "/_mode_E"]
+        mh = s.data[self.name + "/_mode_H"]
+        em = me[k if me.shape[0] > 1 else 0]
+        hm = mh[k if mh.shape[0] > 1 else 0]
+        integrand = (
+            np.cross(em, ph[3:].conj(), axis=0) + np.cross(ph[:3].conj(), hm, axis=0)
+        )[self.axis]
+        alpha = np.sum(integrand * self.area_numpy) / 4
+        return float(abs(alpha) ** 2)
+
+
+def attach(solver):
+    """detectors.py:214-220, plus accumulator sharing for identical planes."""
+    for obj in solver.meta["objects"]:
+        if obj["class"].endswith("Detector"):
+            m = Monitor(solver, obj)
+            key = m._key()
+            for other in solver.monitors:
+                if other.shared is None and other._key() == key:
+                    m.shared = other
+                    m.phasor = other.phasor
+                    m.flux = other.flux
+                    break
+            solver.monitors.append(m)
+            if m.exact:
+                solver.save_h_from = min(solver.save_h_from, m.first)
+
+
+def measurements(solver, k=0):
+    """detectors.py:223-232 at frequency index k; with K > 1 frequencies the
+    per-frequency values are added as `<name>_spectrum` lists."""
+    modal = [m for m in solver.monitors if m.obj["class"] == "ModeOverlapDetector"]
+    powers = {m.name: m.power(solver, k) for m in modal}
+    if powers:
+        powers["modal_transmission"] = powers["mode_out"] / powers["mode_in"]
+        if "mode_reflected" in powers:
+            powers["modal_reflection"] = powers["mode_reflected"] / powers["mode_in"]
+        K = min(len(m.frequencies) for m in modal)
+        if K > 1:
+            for m in modal:
+                powers[m.name + "_spectrum"] = [m.power(solver, j) for j in range(K)]
+            powers["modal_transmission_spectrum"] = [
+                a / b for a, b in zip(powers["mode_out_spectrum"], powers["mode_in_spectrum"])
+            ]
+            powers["frequencies_hz"] = modal[0].frequencies[:K]
+    return powers

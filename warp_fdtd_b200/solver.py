@@ -1,0 +1,415 @@
+"""Drop-in for warp_fdtd/solver.py: fixed-input 3-D FDTD on the B200.
+
+Same constructor, validation (ValueError messages), attributes and methods as
+the reference `Solver` (solver.py:53-264).  What changes underneath:
+
+* one fused E+H kernel per step (csrc/step_fused.cu) instead of two sweeps;
+  fields and CPML state ping-pong between two buffers, so `E`, `H` and `hprev`
+  are views of the buffer the step counter's parity selects and no hprev copy
+  is ever written;
+* materials are stored as uint8 indices into an inverse-permittivity table
+  when the grid has at most 256 distinct values (material="auto"), else as
+  float32 per cell;
+* detectors accumulate K-frequency DFTs in float64 (detectors.py);
+* graphs are torch CUDA graphs of `graph_steps` fused steps.
+All device memory is torch tensors; every kernel runs through the C ABI.
+"""
+
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import kernels as k
+from ._lib import ptr
+from .bundle import read_bundle
+
+C0 = 299792458.0
+
+
+def pack_coefficients(coeff, shape):
+    """solver.py:16-29: rank active planes per axis; pad six histories to the largest slab.
+
+    Returns the (3, L, 4) table whose last column is the small exact integer
+    plane rank, and the packed psi column count."""
+    packed = np.zeros((*coeff.shape[:2], 4), np.float32)
+    packed[..., :3] = coeff
+    slab_sizes = []
+    for axis, length in enumerate(shape):
+        active = coeff[axis, :length, 0] != 0
+        packed[axis, :length, 3] = np.maximum(np.cumsum(active) - 1, 0)
+        slab_sizes.append(int(active.sum()) * (int(np.prod(shape)) // length))
+    return packed, max(1, *slab_sizes)
+
+
+def owned_array_bytes(solver):
+    """solver.py:32-50: live owned device-tensor storage (deduplicated by pointer).
+
+    Excludes allocator, graph and driver overhead; not a peak measurement."""
+    seen = set()
+
+    def size(value):
+        if isinstance(value, torch.Tensor):
+            if value.device.type != "cuda":
+                return 0
+            p = value.untyped_storage().data_ptr()
+            if p in seen:
+                return 0
+            seen.add(p)
+            return int(value.untyped_storage().nbytes())
+        if isinstance(value, dict):
+            return sum(size(v) for v in value.values())
+        if isinstance(value, (list, tuple)):
+            return sum(size(v) for v in value)
+        return 0
+
+    return size(vars(solver)) + sum(size(vars(m)) for m in solver.monitors)
+
+
+def cpml_coefficients(meta, data, shape, field):
+    """solver.py:105-123: coeff[axis, pos] = (a, b, 1/kappa), default (0, 1, 1)."""
+    coeff = np.zeros((3, max(shape), 3), np.float32)
+    coeff[:, :, 1:] = 1
+    covered = np.zeros((3, max(shape)), bool)
+    for obj in meta["objects"]:
+        if obj["class"] != "PerfectlyMatchedLayer":
+            continue
+        name = obj["name"]
+        dims = data[f"{name}/pml_a_{field}"].shape
+        axis = int(np.argmax(dims))
+        lo, hi = obj["grid_slice"][axis]
+        if covered[axis, lo:hi].any():
+            raise ValueError("Overlapping CPML slabs unsupported")
+        covered[axis, lo:hi] = True
+        for j, key in enumerate((f"pml_a_{field}", f"pml_b_{field}", f"inv_kappa_{field}")):
+            coeff[axis, lo:hi, j] = data[f"{name}/{key}"].ravel()
+    return coeff
+
+
+def envelope(src, t):
+    """Source envelope in float32.  SingleFrequencyProfile is the reference's
+    ramp (solver.py:178-180); the two pulse profiles are this repository's
+    extensions for broadband runs."""
+    kind = src["temporal_profile"]
+    if kind == "SingleFrequencyProfile":
+        return np.clip(t / np.float32(src["num_startup_periods"] / src["frequency_hz"]), 0, 1)
+    if kind == "GaussianPulseProfile":
+        u = (t - np.float32(src["pulse_delay_s"])) / np.float32(src["pulse_sigma_s"])
+        return np.exp(np.float32(-0.5) * u * u).astype(np.float32)
+    if kind == "HannPulseProfile":
+        u = (t - np.float32(src["pulse_delay_s"])) / np.float32(src["pulse_width_s"]) + np.float32(0.5)
+        s = np.sin(np.float32(np.pi) * u)
+        return np.where((u >= 0) & (u <= 1), s * s, np.float32(0)).astype(np.float32)
+    raise ValueError(f"Unsupported temporal profile {kind}")
+
+
+SUPPORTED_PROFILES = ("SingleFrequencyProfile", "GaussianPulseProfile", "HannPulseProfile")
+
+
+class Solver:
+    def __init__(self, case, device="cuda:0", graph_steps=64, cpml_storage="full",
+                 material="auto", tile=None, path=0):
+        if cpml_storage not in ("full", "packed"):
+            raise ValueError("cpml_storage must be full or packed")
+        if material not in ("auto", "u8", "f32"):
+            raise ValueError("material must be auto, u8 or f32")
+        self.cpml_storage = cpml_storage
+        self.update_e = k.update_e_packed if cpml_storage == "packed" else k.update_e
+        self.update_h = k.update_h_packed if cpml_storage == "packed" else k.update_h
+        self.path = Path(case)
+        self.meta, self.data = read_bundle(self.path)
+        d, m = self.data, self.meta
+        eps = d["inv_permittivity"]
+        if eps.ndim != 4 or eps.shape[0] != 1 or not np.all(np.isfinite(eps)) or np.any(eps <= 0):
+            raise ValueError("Only finite positive isotropic permittivity is supported")
+        if d["inv_permeability"].ndim != 0 or d["inv_permeability"] != 1:
+            raise ValueError("Only relative permeability 1 is supported")
+        if m["settings"].get("precision", "float32") != "float32":
+            raise ValueError("Only float32 field bundles supported")
+        dx = m["settings"]["spacing_nm"] * 1e-9
+        for axis in "xyz":
+            if not np.allclose(np.diff(d[f"{axis}_edges_m"]), dx, rtol=1e-4, atol=0):
+                raise ValueError("Only uniform cubic grids supported")
+        self.shape = tuple(int(v) for v in eps.shape[1:])
+        self.n = int(np.prod(self.shape))
+        self.steps = int(m["time_steps"])
+        if self.steps < 1 or not np.isfinite(m["dt_s"]) or m["dt_s"] <= 0:
+            raise ValueError("Positive time step and trajectory length required")
+        factor = m["settings"].get("courant_factor", 0.99)
+        if not np.isfinite(factor) or not 0 < factor <= 0.99:
+            raise ValueError("Require 0 < exported CFL factor <= 0.99")
+        expected_dt = factor / np.sqrt(3) * dx / C0
+        if not np.isclose(m["dt_s"], expected_dt, rtol=1e-4, atol=0):
+            raise ValueError("Exported time step disagrees with the declared CFL factor")
+        self.device = torch.device(device)
+        if self.device.type != "cuda":
+            raise ValueError("warp_fdtd_b200 runs on CUDA devices only")
+        self.graph_steps = graph_steps
+        if graph_steps < 1:
+            raise ValueError("graph_steps must be positive")
+        self.courant = factor / np.sqrt(3)
+        self.tile = tuple(tile) if tile else (0, 0, 0)
+        self.path = int(path)
+        dev = self.device
+        f32 = dict(dtype=torch.float32, device=dev)
+        nx, ny, nz = self.shape
+        # z rows padded to 16 B (fields, full psi, inv_eps) and 16 elements
+        # (uint8 material) so the TMA pipeline can address every row; padding
+        # cells stay zero and are never written.
+        self._pitch = (nz + 3) // 4 * 4
+        self._mpitch = (nz + 15) // 16 * 16
+        self._cells = nx * ny * self._pitch
+        self._E = [torch.zeros((3, self._cells), **f32) for _ in range(2)]
+        self._H = [torch.zeros((3, self._cells), **f32) for _ in range(2)]
+        self._issued = 0
+        self.step = torch.zeros(1, dtype=torch.int32, device=dev)
+
+        # materials: uint8 index + table when possible, else float32 per cell
+        flat = np.ascontiguousarray(eps.reshape(-1), np.float32)
+        self.eps = torch.from_numpy(flat).to(dev)
+        table, index = np.unique(flat, return_inverse=True)
+        if material == "u8" and len(table) > 256:
+            raise ValueError("material='u8' needs at most 256 distinct inverse permittivities")
+        self.material = None
+        self.material_table = None
+        self._eps_p = None
+        if material != "f32" and len(table) <= 256:
+            self.material_kind = 1
+            m8 = np.zeros((nx, ny, self._mpitch), np.uint8)
+            m8[..., :nz] = index.astype(np.uint8).reshape(self.shape)
+            self.material = torch.from_numpy(m8.reshape(-1)).to(dev)
+            self.material_table = torch.from_numpy(table.astype(np.float32)).to(dev)
+        else:
+            self.material_kind = 0
+            self._eps_p = torch.zeros(self._cells, **f32)
+            self._sync_eps()
+
+        # CPML tables (solver.py:105-131)
+        self.coeffs, self._coeff4 = {}, {}
+        tables = {f: cpml_coefficients(m, d, self.shape, f) for f in "EH"}
+        packed = {f: pack_coefficients(tables[f], self.shape) for f in "EH"}
+        # one column count serves both fields' psi arrays (the fused kernel
+        # addresses E and H state with the same stride)
+        self._psi_cols = (max(packed["E"][1], packed["H"][1]) if cpml_storage == "packed"
+                          else self._cells)
+        for field in "EH":
+            packed4 = packed[field][0]
+            table = packed4 if cpml_storage == "packed" else tables[field]
+            self.coeffs[field] = torch.from_numpy(table).to(dev)
+            self._coeff4[field] = torch.from_numpy(packed4).to(dev)
+            setattr(self, "_psi_" + field.lower(),
+                    [torch.zeros((6, self._psi_cols), **f32) for _ in range(2)])
+
+        # plane mode source (solver.py:132-182)
+        sources = [o for o in m["objects"] if o["class"] == "ModePlaneSource"]
+        if len(sources) != 1:
+            raise ValueError("Exactly one exported plane mode source required")
+        src = sources[0]
+        if (
+            src["direction"] != "+"
+            or src["propagation_axis"] != 0
+            or src["temporal_profile"] not in SUPPORTED_PROFILES
+        ):
+            raise ValueError("Only +x single-frequency source supported")
+        self.source_x = src["grid_slice"][0][0]
+        if src["grid_slice"] != [
+            [self.source_x, self.source_x + 1],
+            [0, self.shape[1]],
+            [0, self.shape[2]],
+        ]:
+            raise ValueError("Source must span complete yz plane")
+        self.sources, self.waves = {}, {}
+        name = src["name"]
+        if not np.array_equal(d[name + "/_time_step_to_on_idx"], np.arange(self.steps)):
+            raise ValueError("Switched source schedules are not supported")
+        if src["temporal_profile"] == "SingleFrequencyProfile" and src["num_startup_periods"] <= 0:
+            raise ValueError("Source must have a positive startup ramp")
+        for field in "EH":
+            profile = d[f"{name}/_{field}"]
+            if np.iscomplexobj(profile):
+                raise ValueError("Complex source profiles unsupported")
+            self.sources[field] = torch.from_numpy(
+                np.ascontiguousarray(profile.reshape(3, -1), np.float32)).to(dev)
+            offsets = d[f"{name}/_time_offset_{field}"].reshape(3, -1)
+            if not np.all(offsets == offsets[:, :1]):
+                raise ValueError("Spatially varying source delays unsupported")
+            # float32 arithmetic with the separate multiply/divide of solver.py:165-181
+            half_step = np.float32(0.5 if field == "E" else 0.0)
+            t = (
+                np.arange(self.steps, dtype=np.float32)[None, :] + half_step + offsets[:, :1]
+            ) * np.float32(m["dt_s"])
+            period = np.float32(1 / src["frequency_hz"])
+            phase = (
+                np.float32(2 * np.pi) * t / period
+                + np.float32(src["phase_shift"])
+                + np.float32(src["profile_phase_shift"])
+            )
+            wave = envelope(src, t) * np.cos(phase) * np.float32(src["static_amplitude_factor"])
+            self.waves[field] = torch.from_numpy(np.ascontiguousarray(wave, np.float32)).to(dev)
+        self.monitors = []
+        self.save_h_from = self.steps
+        self.graphs = {}
+        self._args = self._step_args()
+
+    # -- buffers selected by the number of issued steps --------------------
+    def _compact(self, buf, rows):
+        """(rows, n) view of a padded buffer (a copy when rows are padded)."""
+        if self._pitch == self.shape[2]:
+            return buf
+        nx, ny, nz = self.shape
+        return buf.view(rows, nx, ny, self._pitch)[..., :nz].reshape(rows, self.n)
+
+    @property
+    def E(self):
+        return self._compact(self._E[self._issued & 1], 3)
+
+    @property
+    def H(self):
+        return self._compact(self._H[self._issued & 1], 3)
+
+    @property
+    def hprev(self):
+        """H(n-1/2) after the last issued step (zeros before the first)."""
+        return self._compact(self._H[(self._issued + 1) & 1], 3)
+
+    @property
+    def psi_e(self):
+        buf = self._psi_e[self._issued & 1]
+        return buf if self.cpml_storage == "packed" else self._compact(buf, 6)
+
+    @property
+    def psi_h(self):
+        buf = self._psi_h[self._issued & 1]
+        return buf if self.cpml_storage == "packed" else self._compact(buf, 6)
+
+    def _sync_eps(self):
+        """Copy `eps` (n,) into the padded float32 material the kernel reads."""
+        nx, ny, nz = self.shape
+        self._eps_p.view(nx, ny, self._pitch)[..., :nz].copy_(self.eps.view(nx, ny, nz))
+
+    def _step_args(self):
+        a = _lib.StepArgs()
+        for j in range(2):
+            a.E[j] = ptr(self._E[j])
+            a.H[j] = ptr(self._H[j])
+            a.psi_e[j] = ptr(self._psi_e[j])
+            a.psi_h[j] = ptr(self._psi_h[j])
+        a.psi_cols = self._psi_cols
+        a.coeff_e = ptr(self._coeff4["E"])
+        a.coeff_h = ptr(self._coeff4["H"])
+        a.clen = int(self._coeff4["E"].shape[1])
+        a.packed = int(self.cpml_storage == "packed")
+        a.material_kind = self.material_kind
+        if self.material_kind == 0:
+            a.inv_eps = ptr(self._eps_p)
+        if self.material_kind == 1:
+            a.material = ptr(self.material)
+            a.material_table = ptr(self.material_table)
+            a.material_count = int(self.material_table.numel())
+        a.src_e = ptr(self.sources["E"])
+        a.src_h = ptr(self.sources["H"])
+        a.waves_e = ptr(self.waves["E"])
+        a.waves_h = ptr(self.waves["H"])
+        a.waves_cols = self.steps
+        a.source_x = int(self.source_x)
+        a.courant = float(self.courant)
+        a.step = ptr(self.step)
+        a.nx, a.ny, a.nz = self.shape
+        a.pitch_z = self._pitch
+        a.material_pitch = self._mpitch
+        a.tile_y, a.tile_z, a.chunk_x = (int(v) for v in self.tile)
+        a.path = int(self.path)
+        return a
+
+    def set_tile(self, tile_y, tile_z, chunk_x=0):
+        """Change the fused kernel's launch shape; captured graphs are dropped."""
+        self.tile = (int(tile_y), int(tile_z), int(chunk_x))
+        self._args = self._step_args()
+        self.graphs = {}
+
+    def set_path(self, path):
+        """0 auto, 1 shared-memory staging, 2 TMA pipeline; drops captured graphs."""
+        self.path = int(path)
+        self._args = self._step_args()
+        self.graphs = {}
+
+    def refresh_material(self):
+        """Propagate an in-place change of `eps` to the copy the fused kernel reads."""
+        if self.material_kind != 0:
+            raise ValueError("refresh_material needs material='f32'")
+        self._sync_eps()
+
+    def reset(self):
+        for group in (self._E, self._H, self._psi_e, self._psi_h):
+            for a in group:
+                a.zero_()
+        self.step.zero_()
+        self._issued = 0
+        for monitor in self.monitors:
+            monitor.reset()
+        torch.cuda.synchronize(self.device)
+
+    def launch_step(self):
+        """One step: fused E+H update, detectors, advance (solver.py:194-237)."""
+        if self._issued >= self.steps and not torch.cuda.is_current_stream_capturing():
+            raise ValueError("Trajectory complete; call reset() before stepping again")
+        stream = _lib.stream_handle(self.device)
+        _lib.call("fdtd_step_fused", self._args, stream)
+        for monitor in self.monitors:
+            monitor.launch(self)
+        _lib.call("fdtd_advance", ptr(self.step), 1, stream)
+        self._issued += 1
+
+    def compile(self):
+        start = time.perf_counter()
+        with torch.cuda.device(self.device):
+            self.launch_step()
+            torch.cuda.synchronize(self.device)
+            self.reset()
+            for length in {self.graph_steps, self.steps % self.graph_steps} - {0}:
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, capture_error_mode="relaxed"):
+                    for _ in range(length):
+                        self.launch_step()
+                self._issued -= length
+                self.graphs[length] = g
+            self.reset()
+        return time.perf_counter() - start
+
+    def run(self):
+        with torch.cuda.device(self.device):
+            if not self.graphs:
+                for _ in range(self.steps - self._issued):
+                    self.launch_step()
+            else:
+                for _ in range(self.steps // self.graph_steps):
+                    self.graphs[self.graph_steps].replay()
+                tail = self.steps % self.graph_steps
+                if tail:
+                    self.graphs[tail].replay()
+                self._issued += self.steps
+            torch.cuda.synchronize(self.device)
+
+    def fields(self):
+        return {
+            name: arr.cpu().numpy().reshape(3, *self.shape)
+            for name, arr in [("E", self.E), ("H", self.H)]
+        }
+
+    def set_fields(self, E=None, H=None):
+        """Load (3, n) or (3, nx, ny, nz) fields into the current buffers."""
+        nx, ny, nz = self.shape
+        for arr, bufs in ((E, self._E), (H, self._H)):
+            if arr is None:
+                continue
+            src = torch.as_tensor(np.asarray(arr, np.float32)).reshape(3, nx, ny, nz)
+            dst = bufs[self._issued & 1].view(3, nx, ny, self._pitch)
+            dst[..., :nz].copy_(src.to(self.device))
+
+    def summary(self):
+        return json.dumps({"shape": self.shape, "steps": self.steps,
+                           "material_kind": self.material_kind,
+                           "cpml_storage": self.cpml_storage})
