@@ -142,19 +142,35 @@ int fdtd_material_smooth_adjoint(const float *g, const float *weights, int radiu
  * Rows may be padded: cell (x, y, z) of a field, of full-storage psi and of
  * inv_eps lives at (x*ny + y)*pitch_z + z, and of the uint8 material at
  * (x*ny + y)*material_pitch + z.  Padding cells must hold zeros (fields) and
- * are never written.  The TMA pipeline (path 2) needs pitch_z % 4 == 0,
- * material_pitch % 16 == 0 and 16-byte aligned buffers; path 0 picks it
- * whenever those hold and falls back to the shared-memory path (1). */
+ * are never written.  The TMA paths need pitch_z % 4 == 0, material_pitch % 16
+ * == 0 and 16-byte aligned buffers; path 3 also needs pitch_z <= 248 and the
+ * slab psi layout.  Path 0 picks 3, then 2, then the shared-memory path 1. */
+/* CPML state layouts of fdtd_step_args.packed:
+ *  FDTD_PSI_FULL   (6, psi_cols) indexed by cell (solver.py cpml_storage="full");
+ *  FDTD_PSI_PACKED (6, psi_cols) indexed by the reference's plane-rank formula
+ *                  (kernels.py:50-74, cpml_storage="packed");
+ *  FDTD_PSI_SLAB   per field one buffer holding three slab blocks, rows padded
+ *                  to pitch_z: X [2][psi_rx][ny][pitch_z], then
+ *                  Y [2][psi_ry][nx][pitch_z], then Z [2][nx][ny][psi_rz]
+ *                  (psi_rz a multiple of 4); the slot pair of each axis is
+ *                  (2*axis, 2*axis+1) and ranks come from coeff[...][3].  The
+ *                  Z block is contiguous in z-rank so the full-z TMA path can
+ *                  stage it with the fields. */
+#define FDTD_PSI_FULL 0
+#define FDTD_PSI_PACKED 1
+#define FDTD_PSI_SLAB 2
+
 typedef struct fdtd_step_args {
     float *E[2];
     float *H[2];
     float *psi_e[2];           /* (6, psi_cols) each */
     float *psi_h[2];
-    long long psi_cols;        /* nx*ny*pitch_z (full storage) or packed slab size */
+    long long psi_cols;        /* layouts 0/1: columns of each (6, psi_cols) psi array */
     const float *coeff_e;      /* (3, clen, 4): a, b, 1/kappa, packed plane rank */
     const float *coeff_h;
     int clen;
-    int packed;                /* 0: psi indexed by cell, 1: by packed plane rank */
+    int packed;                /* psi layout, see FDTD_PSI_* */
+    int psi_rx, psi_ry, psi_rz; /* slab layout: active positions per axis (max of E, H) */
     int material_kind;         /* 0: inv_eps per cell, 1: uint8 index into table */
     const float *inv_eps;      /* per cell float32, material_kind 0 */
     const uint8_t *material;   /* per cell uint8, material_kind 1 */
@@ -172,7 +188,10 @@ typedef struct fdtd_step_args {
     int pitch_z;               /* 0: nz */
     int material_pitch;        /* 0: nz */
     int tile_y, tile_z, chunk_x; /* launch shape; 0 picks defaults */
-    int path;                  /* 0 auto, 1 shared-memory staging, 2 TMA pipeline */
+    int path;                  /* 0 auto, 1 shared-memory staging, 2 TMA pipeline (tiled z),
+                                  3 TMA pipeline over full-z tiles (needs FDTD_PSI_SLAB) */
+    int vector;                /* TMA path: z cells per thread (1, 2, 4); 0 picks */
+    int stages;                /* TMA path: planes in the load ring (2..8); 0 picks */
     int *error;                /* optional device int, set to 1 if a bounded wait expires */
 } fdtd_step_args;
 

@@ -35,6 +35,9 @@ class StepArgs(ctypes.Structure):
         ("coeff_h", _p),
         ("clen", _i),
         ("packed", _i),
+        ("psi_rx", _i),
+        ("psi_ry", _i),
+        ("psi_rz", _i),
         ("material_kind", _i),
         ("inv_eps", _p),
         ("material", _p),
@@ -57,6 +60,8 @@ class StepArgs(ctypes.Structure):
         ("tile_z", _i),
         ("chunk_x", _i),
         ("path", _i),
+        ("vector", _i),
+        ("stages", _i),
         ("error", _p),
     ]
 

@@ -307,7 +307,11 @@ extern "C" int fdtd_step_fused(const fdtd_step_args *args, void *stream) {
             return FDTD_ERR_ARG;
         }
     }
-    if (!a.packed && a.psi_cols < (long long)a.nx * a.ny * a.pitch_z) {
+    if (a.packed < 0 || a.packed > 2) {
+        set_error("fdtd_step_fused: unknown psi layout %d", a.packed);
+        return FDTD_ERR_ARG;
+    }
+    if (a.packed == FDTD_PSI_FULL && a.psi_cols < (long long)a.nx * a.ny * a.pitch_z) {
         set_error("fdtd_step_fused: full CPML storage needs psi_cols >= nx*ny*pitch_z");
         return FDTD_ERR_ARG;
     }
@@ -330,17 +334,49 @@ extern "C" int fdtd_step_fused(const fdtd_step_args *args, void *stream) {
         return FDTD_ERR_ARG;
     }
     int path = a.path;
+    if (a.packed == FDTD_PSI_SLAB) {
+        // the slab layout is only read by the full-z pipeline
+        if (path != 0 && path != 3) {
+            set_error("fdtd_step_fused: the slab psi layout needs path 3");
+            return FDTD_ERR_ARG;
+        }
+        if (!fz_eligible(a)) {
+            set_error("fdtd_step_fused: full-z path needs pitch_z %% 4 == 0, pitch_z <= 248, "
+                      "psi_rz %% 4 == 0 and 16-byte aligned buffers");
+            return FDTD_ERR_ARG;
+        }
+        path = 3;
+    } else if (path == 3) {
+        set_error("fdtd_step_fused: path 3 needs the slab psi layout");
+        return FDTD_ERR_ARG;
+    }
     if (path == 0) path = tma_eligible(a) ? 2 : 1;
     if (path == 2 && !tma_eligible(a)) {
         set_error("fdtd_step_fused: TMA path needs pitch_z %% 4 == 0, material_pitch %% 16 == 0 "
                   "and 16-byte aligned buffers");
         return FDTD_ERR_ARG;
     }
-    if (path != 1 && path != 2) {
-        set_error("fdtd_step_fused: path must be 0, 1 or 2");
+    if (path != 1 && path != 2 && path != 3) {
+        set_error("fdtd_step_fused: path must be 0, 1, 2 or 3");
         return FDTD_ERR_ARG;
     }
     cudaStream_t st = (cudaStream_t)stream;
+    if (path == 3) {
+        if (a.tile_y <= 0) a.tile_y = 5;
+        const int tiles = (a.ny + a.tile_y - 1) / a.tile_y;
+        if (a.chunk_x <= 0) {
+            // about three waves of two resident blocks per SM, chunks of >= 16 planes
+            int want = 148 * 2 * 3;
+            int chunks = (want + tiles - 1) / tiles;
+            a.chunk_x = (a.nx + chunks - 1) / chunks;
+            if (a.chunk_x < 16) a.chunk_x = 16 < a.nx ? 16 : a.nx;
+        }
+        if (a.tile_y < 1 || a.chunk_x < 1) {
+            set_error("fdtd_step_fused: invalid tile");
+            return FDTD_ERR_ARG;
+        }
+        return launch_fz(a, st);
+    }
     if (path == 2) {
         if (a.tile_z <= 0) {
             // uint8 material boxes must start on 16-byte boundaries: tile_z % 16 == 0

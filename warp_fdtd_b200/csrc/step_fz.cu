@@ -1,0 +1,585 @@
+// Fused Yee leapfrog step over full-z tiles (path 3, the Solver's default).
+//
+// A block owns rows [y0, y0 + tile_y) of the y-z plane across the whole z
+// extent and a chunk of x planes, marching along x with the E update one
+// plane ahead of the H update (same scheme and arithmetic as step_fused.cu /
+// step_tma.cu).  Because a tile spans all of z there is no z halo: the -z
+// neighbour of z = 0 and the +z neighbour of z = nz - 1 are the grid's zero
+// padding.  Each plane is staged by TMA in one ring stage:
+//
+//   H(p)   rows y0-1 .. y0+ty, z from -4 (box width pitch + 4; the -4 keeps
+//          the box start 16-byte aligned and supplies z = -1 as zero fill)
+//   E(p)   rows y0 .. y0+ty, z 0 .. pitch
+//   material, and the z-slab CPML state of E (rows y0..y0+ty) and H (rows
+//   y0..y0+ty-1), which the slab layout keeps contiguous in z-rank.
+//
+// A thread handles four consecutive z cells of one row (128-bit shared-memory
+// loads and global stores) for both updates, so index arithmetic is hoisted
+// out of the plane loop.  x- and y-slab CPML state is read directly (float4,
+// coalesced) only in the planes / rows where it is active; whether a cell
+// group takes the CPML branch is decided per thread from tile coefficient
+// tables in shared memory.  Outside the slabs the reference's 1 * d == d, so
+// the plain difference is used, bit for bit identical.
+#include "common.cuh"
+#include "step_internal.h"
+#include "tma_util.cuh"
+
+namespace wfb {
+
+struct FzLayout {
+    int ty, P, HB, MB, RZ, S;
+    int off_h, off_e, off_m, off_pze, off_pzh;  // byte offsets inside a stage
+    int stage_bytes;
+    unsigned tx_bytes;
+    int off_stages, off_ring, RW, off_coef, off_mtab, smem_bytes;
+};
+
+struct FzMaps {
+    CUtensorMap E[2], H[2], M, PZE[2], PZH[2];
+};
+
+struct FzParams {
+    fdtd_step_args a;
+    FzLayout L;
+    long long xoff, yoff, zoff;  // slab-block offsets (elements) inside a psi buffer
+};
+
+__device__ __forceinline__ bool active(float4 c) { return c.x != 0.0f || c.z != 1.0f; }
+
+// V consecutive floats held in registers (V = 2 or 4 z cells per thread).
+template <int V>
+struct VF {
+    float v[V];
+};
+
+template <int V>
+__device__ __forceinline__ VF<V> ldsv(const float *p) {
+    VF<V> r;
+    if constexpr (V == 4) {
+        const float4 t = *(const float4 *)p;
+        r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+    } else {
+        const float2 t = *(const float2 *)p;
+        r.v[0] = t.x; r.v[1] = t.y;
+    }
+    return r;
+}
+
+template <int V>
+__device__ __forceinline__ VF<V> ldgv(const float *p) {
+    VF<V> r;
+    if constexpr (V == 4) {
+        const float4 t = __ldg((const float4 *)p);
+        r.v[0] = t.x; r.v[1] = t.y; r.v[2] = t.z; r.v[3] = t.w;
+    } else {
+        const float2 t = __ldg((const float2 *)p);
+        r.v[0] = t.x; r.v[1] = t.y;
+    }
+    return r;
+}
+
+template <int V>
+__device__ __forceinline__ void stv(float *p, const VF<V> &r) {
+    if constexpr (V == 4)
+        *(float4 *)p = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+    else
+        *(float2 *)p = make_float2(r.v[0], r.v[1]);
+}
+
+template <int V>
+__device__ __forceinline__ VF<V> zero_v() {
+    VF<V> r;
+#pragma unroll
+    for (int j = 0; j < V; ++j) r.v[j] = 0.0f;
+    return r;
+}
+
+// kernels.py:29-47 applied to one difference with its old psi value.
+__device__ __forceinline__ float cpml1(float d, float4 c, float psi_old, float &psi_new) {
+    if (c.x != 0.0f) {
+        const float p = c.y * psi_old + c.x * d;
+        psi_new = p;
+        return c.z * d + p;
+    }
+    return c.z * d;
+}
+
+// CPML filter of the two differences an axis owns, for a cell group whose
+// coefficient c is uniform (x: the plane, y: the row); psi in a slab block
+// at `ib` (slot stride `slot`), read from `po`, written to `pn` if `own`.
+template <int V>
+__device__ __forceinline__ void cpml_axis(VF<V> &d0, VF<V> &d1, float4 c, const float *po,
+                                          float *pn, i64 ib, i64 slot, bool own) {
+    VF<V> p0 = zero_v<V>(), p1 = zero_v<V>(), n0 = zero_v<V>(), n1 = zero_v<V>();
+    if (c.x != 0.0f) {
+        p0 = ldgv<V>(po + ib);
+        p1 = ldgv<V>(po + ib + slot);
+    }
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+        d0.v[j] = cpml1(d0.v[j], c, p0.v[j], n0.v[j]);
+        d1.v[j] = cpml1(d1.v[j], c, p1.v[j], n1.v[j]);
+    }
+    if (own && c.x != 0.0f) {
+        stv<V>(pn + ib, n0);
+        stv<V>(pn + ib + slot, n1);
+    }
+}
+
+template <int MAT, int S, int V>
+__global__ void __launch_bounds__(512)
+    fz_step_kernel(const __grid_constant__ FzMaps maps, const __grid_constant__ FzParams prm) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    const fdtd_step_args &a = prm.a;
+    const FzLayout &L = prm.L;
+    const int nx = a.nx, ny = a.ny, nz = a.nz, P = L.P, TY = L.ty;
+    const i64 cols = (i64)nx * ny * P;
+    const i64 plane = (i64)ny * P;
+    const int HB = L.HB, RW = L.RW, RZ = L.RZ;
+    const int HS = (TY + 2) * HB;   // H component stride in a stage
+    const int ES = (TY + 1) * P;    // E component stride in a stage
+    const int RS = (TY + 1) * RW;   // ring component stride
+
+    uint64_t *bars = (uint64_t *)smem;
+    unsigned char *stage0 = smem + L.off_stages;
+    float *ring = (float *)(smem + L.off_ring);  // [2][3][TY+1][RW]
+    float4 *cey = (float4 *)(smem + L.off_coef);
+    float4 *chy = cey + (TY + 1);
+    float4 *cez = chy + (TY + 1);
+    float4 *chz = cez + P;
+    float *mtab = (float *)(smem + L.off_mtab);
+
+    const int tiles_y = (ny + TY - 1) / TY;
+    const int tyi = blockIdx.x % tiles_y;
+    const int chunk = blockIdx.x / tiles_y;
+    const int y0 = tyi * TY;
+    const int xa = chunk * a.chunk_x;
+    if (xa >= nx) return;
+    const int xb = min(xa + a.chunk_x, nx);
+    const int last = xb - xa + 1;  // planes k = 0..last are xa-1 .. xb
+
+    const int t = a.step[0];
+    const int s = t & 1;
+    float *__restrict__ En = a.E[s ^ 1];
+    float *__restrict__ Hn = a.H[s ^ 1];
+    const float *__restrict__ pe_o = a.psi_e[s];
+    float *__restrict__ pe_n = a.psi_e[s ^ 1];
+    const float *__restrict__ ph_o = a.psi_h[s];
+    float *__restrict__ ph_n = a.psi_h[s ^ 1];
+    const float4 *__restrict__ ce = (const float4 *)a.coeff_e;
+    const float4 *__restrict__ ch = (const float4 *)a.coeff_h;
+    const int clen = a.clen;
+    const float courant = a.courant;
+    const int lx = threadIdx.x, ly = threadIdx.y;
+    const int tid = ly * blockDim.x + lx, nth = blockDim.x * blockDim.y;
+    const int zv = lx * V;        // first of this thread's V z cells
+    const int gy = y0 + ly;       // this thread's row (E: ly <= TY, H: ly < TY)
+    const bool wave_ok = t >= 0 && t < a.waves_cols;
+    const i64 xslot = (i64)a.psi_rx * plane;      // slot stride of the X block
+    const i64 yslot = (i64)a.psi_ry * nx * P;     // ... of the Y block
+    const i64 zslot = (i64)nx * ny * RZ;          // ... of the Z block
+
+    auto stage_ptr = [&](int k) { return stage0 + (size_t)(k % S) * L.stage_bytes; };
+    auto issue = [&](int k) {
+        unsigned char *st = stage_ptr(k);
+        uint64_t *bar = bars + (k % S);
+        const int p = xa - 1 + k;
+        mbar_expect_tx(bar, L.tx_bytes);
+        tma_load_4d(st + L.off_h, &maps.H[s], -4, y0 - 1, p, 0, bar);
+        tma_load_4d(st + L.off_e, &maps.E[s], 0, y0, p, 0, bar);
+        tma_load_3d(st + L.off_m, &maps.M, 0, y0, p, bar);
+        if (RZ > 0) {
+            tma_load_4d(st + L.off_pze, &maps.PZE[s], 0, y0, p, 0, bar);
+            tma_load_4d(st + L.off_pzh, &maps.PZH[s], 0, y0, p, 0, bar);
+        }
+    };
+
+    if (tid == 0) {
+        for (int j = 0; j < S; ++j) mbar_init(bars + j, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (MAT == 1)
+        for (int j = tid; j < 256; j += nth) mtab[j] = j < a.material_count ? a.material_table[j] : 0.0f;
+    const float4 ident = make_float4(0.f, 1.f, 1.f, 0.f);
+    for (int j = tid; j <= TY; j += nth) {
+        const int y = y0 + j;
+        cey[j] = y < ny ? __ldg(ce + clen + y) : ident;
+        chy[j] = y < ny ? __ldg(ch + clen + y) : ident;
+    }
+    for (int j = tid; j < P; j += nth) {
+        cez[j] = j < nz ? __ldg(ce + 2 * clen + j) : ident;
+        chz[j] = j < nz ? __ldg(ch + 2 * clen + j) : ident;
+    }
+    // the ring's +z pad columns (z = P .. P+3) are the zero padding beyond the grid
+    for (int j = tid; j < 2 * 3 * (TY + 1) * 4; j += nth) {
+        const int r = j >> 2, c = j & 3;
+        ring[r * RW + P + c] = 0.0f;
+    }
+    __syncthreads();
+    // per-thread CPML activity of its row and its z cells
+    const float4 my_cey = cey[ly], my_chy = chy[min(ly, TY - 1)];
+    const bool yE = active(my_cey), yH = ly < TY && active(my_chy);
+    bool zE = false, zH = false;
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+        zE |= active(cez[zv + j]);
+        zH |= active(chz[zv + j]);
+    }
+
+    int issued;
+    if (tid == 0)
+        for (int k = 0; k <= last && k < S; ++k) issue(k);
+    issued = min(last, S - 1);
+    const long limit = 1L << 24;
+    bool timed_out = false;
+    int done = -1;
+    if (mbar_wait_bounded(bars, 0, limit))
+        done = 0;
+    else
+        timed_out = true;
+
+    const int h_off = (ly + 1) * HB + zv + 4;  // this cell group in an H box
+    const int e_off = ly * P + zv;             // ... in an E box
+    const int r_off = ly * RW + zv;            // ... in the E ring
+    const int g_off = gy * P + zv;             // ... in a field plane (elements)
+    const bool row_in = gy < ny;
+
+    int k = 1;
+    for (; k <= last; ++k) {
+        const int p = xa - 1 + k;
+        if (!timed_out) {
+            if (mbar_wait_bounded(bars + (k % S), (k / S) & 1, limit))
+                done = k;
+            else
+                timed_out = true;
+        }
+        const unsigned char *stc = stage_ptr(k);
+        const unsigned char *stp = stage_ptr(k - 1);
+        float *Rc = ring + (k & 1) * 3 * RS;
+        // ---------------- E update, rows y0 .. y0+TY ----------------
+        if (!timed_out) {
+            VF<V> o[3] = {zero_v<V>(), zero_v<V>(), zero_v<V>()};
+            if (p < nx && row_in) {
+                const float *Hc = (const float *)(stc + L.off_h);
+                const float *Hp = (const float *)(stp + L.off_h);
+                const float *Eo = (const float *)(stc + L.off_e);
+                VF<V> dx[3], dy[3], dz[3];
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    const VF<V> hc = ldsv<V>(Hc + q * HS + h_off);
+                    const VF<V> hp = ldsv<V>(Hp + q * HS + h_off);
+                    const VF<V> hy = ldsv<V>(Hc + q * HS + h_off - HB);
+                    float zm = Hc[q * HS + h_off - 1];
+#pragma unroll
+                    for (int j = 0; j < V; ++j) {
+                        dx[q].v[j] = hc.v[j] - hp.v[j];
+                        dy[q].v[j] = hc.v[j] - hy.v[j];
+                        dz[q].v[j] = hc.v[j] - zm;
+                        zm = hc.v[j];
+                    }
+                }
+                float ie[V];
+                if (MAT == 1) {
+                    const unsigned char *m = stc + L.off_m + ly * L.MB + zv;
+                    if constexpr (V == 4) {
+                        const uchar4 mm = *(const uchar4 *)m;
+                        ie[0] = mtab[mm.x]; ie[1] = mtab[mm.y]; ie[2] = mtab[mm.z]; ie[3] = mtab[mm.w];
+                    } else {
+                        const uchar2 mm = *(const uchar2 *)m;
+                        ie[0] = mtab[mm.x]; ie[1] = mtab[mm.y];
+                    }
+                } else {
+                    const VF<V> t4 = ldsv<V>((const float *)(stc + L.off_m) + ly * L.MB + zv);
+#pragma unroll
+                    for (int j = 0; j < V; ++j) ie[j] = t4.v[j];
+                }
+                const float4 cx = __ldg(ce + p);
+                const bool own = p < xb && ly < TY;
+                // CPML filter per axis (kernels.py:113-118): x is uniform over the
+                // block's plane, y over the thread's row, z only in slab lanes.
+                // dx[2] = dxz, dx[1] = dxy, dy[0] = dyx, dy[2] = dyz, dz[1] = dzy, dz[0] = dzx
+                if (active(cx))
+                    cpml_axis<V>(dx[2], dx[1], cx, pe_o, pe_n,
+                                 prm.xoff + ((i64)(int)cx.w * ny + gy) * P + zv, xslot, own);
+                if (yE)
+                    cpml_axis<V>(dy[0], dy[2], my_cey, pe_o, pe_n,
+                                 prm.yoff + ((i64)(int)my_cey.w * nx + p) * P + zv, yslot, own);
+                if (zE) {
+                    const float *pz = (const float *)(stc + L.off_pze);  // [2][TY+1][RZ]
+#pragma unroll
+                    for (int j = 0; j < V; ++j) {
+                        const float4 cz = cez[zv + j];
+                        float z4 = 0.0f, z5 = 0.0f, u4 = 0.f, u5 = 0.f;
+                        const int rz = (int)cz.w;
+                        if (cz.x != 0.0f) {
+                            z4 = pz[ly * RZ + rz];
+                            z5 = pz[(TY + 1) * RZ + ly * RZ + rz];
+                        }
+                        dz[1].v[j] = cpml1(dz[1].v[j], cz, z4, u4);
+                        dz[0].v[j] = cpml1(dz[0].v[j], cz, z5, u5);
+                        if (own && cz.x != 0.0f && zv + j < nz) {
+                            const i64 zb = prm.zoff + ((i64)p * ny + gy) * RZ + rz;
+                            pe_n[zb] = u4;
+                            pe_n[zb + zslot] = u5;
+                        }
+                    }
+                }
+                const VF<V> e0 = ldsv<V>(Eo + e_off), e1 = ldsv<V>(Eo + ES + e_off),
+                            e2 = ldsv<V>(Eo + 2 * ES + e_off);
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    const float iej = ie[j];
+                    float v0 = e0.v[j] + (courant * (dy[2].v[j] - dz[1].v[j])) * iej;
+                    float v1 = e1.v[j] + (courant * (dz[0].v[j] - dx[2].v[j])) * iej;
+                    float v2 = e2.v[j] + (courant * (dx[1].v[j] - dy[0].v[j])) * iej;
+                    const int gz = zv + j;
+                    if (p == a.source_x && wave_ok && gz < nz) {
+                        const i64 sidx = (i64)gy * nz + gz;
+                        const i64 syz = (i64)ny * nz;
+                        v1 = v1 + ((a.src_h[2 * syz + sidx] * a.waves_h[2 * a.waves_cols + t]) * courant) * iej;
+                        v2 = v2 - ((a.src_h[syz + sidx] * a.waves_h[a.waves_cols + t]) * courant) * iej;
+                    }
+                    const bool in = gz < nz;
+                    o[0].v[j] = in ? v0 : 0.0f;
+                    o[1].v[j] = in ? v1 : 0.0f;
+                    o[2].v[j] = in ? v2 : 0.0f;
+                }
+                if (own) {
+                    float *dst = En + (i64)p * plane + g_off;
+                    stv<V>(dst, o[0]);
+                    stv<V>(dst + cols, o[1]);
+                    stv<V>(dst + 2 * cols, o[2]);
+                }
+            }
+            stv<V>(Rc + r_off, o[0]);
+            stv<V>(Rc + RS + r_off, o[1]);
+            stv<V>(Rc + 2 * RS + r_off, o[2]);
+        }
+        if (__syncthreads_or(timed_out)) {
+            timed_out = true;
+            break;
+        }
+        // ---------------- H update at plane q = p - 1, rows y0 .. y0+TY-1 ----------------
+        const int q = p - 1;
+        if (q >= xa && ly < TY && row_in) {
+            const float *Rq = ring + ((k - 1) & 1) * 3 * RS;
+            VF<V> dx[3], dy[3], dz[3];
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const VF<V> eq = ldsv<V>(Rq + r * RS + r_off);
+                const VF<V> ep = ldsv<V>(Rc + r * RS + r_off);
+                const VF<V> eyp = ldsv<V>(Rq + r * RS + r_off + RW);
+                const float zp = Rq[r * RS + r_off + V];
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    const float nxt = j + 1 < V ? eq.v[j + 1 < V ? j + 1 : 0] : zp;
+                    dx[r].v[j] = ep.v[j] - eq.v[j];
+                    dy[r].v[j] = eyp.v[j] - eq.v[j];
+                    dz[r].v[j] = nxt - eq.v[j];
+                }
+            }
+            const float4 cx = __ldg(ch + q);
+            if (active(cx))
+                cpml_axis<V>(dx[2], dx[1], cx, ph_o, ph_n,
+                             prm.xoff + ((i64)(int)cx.w * ny + gy) * P + zv, xslot, true);
+            if (yH)
+                cpml_axis<V>(dy[0], dy[2], my_chy, ph_o, ph_n,
+                             prm.yoff + ((i64)(int)my_chy.w * nx + q) * P + zv, yslot, true);
+            if (zH) {
+                const float *pz = (const float *)(stp + L.off_pzh);  // [2][TY][RZ]
+#pragma unroll
+                for (int j = 0; j < V; ++j) {
+                    const float4 cz = chz[zv + j];
+                    float z4 = 0.0f, z5 = 0.0f, u4 = 0.f, u5 = 0.f;
+                    const int rz = (int)cz.w;
+                    if (cz.x != 0.0f) {
+                        z4 = pz[ly * RZ + rz];
+                        z5 = pz[TY * RZ + ly * RZ + rz];
+                    }
+                    dz[1].v[j] = cpml1(dz[1].v[j], cz, z4, u4);
+                    dz[0].v[j] = cpml1(dz[0].v[j], cz, z5, u5);
+                    if (cz.x != 0.0f && zv + j < nz) {
+                        const i64 zb = prm.zoff + ((i64)q * ny + gy) * RZ + rz;
+                        ph_n[zb] = u4;
+                        ph_n[zb + zslot] = u5;
+                    }
+                }
+            }
+            const float *Hq = (const float *)(stp + L.off_h);
+            const VF<V> h0 = ldsv<V>(Hq + h_off), h1 = ldsv<V>(Hq + HS + h_off),
+                        h2 = ldsv<V>(Hq + 2 * HS + h_off);
+            VF<V> o[3];
+#pragma unroll
+            for (int j = 0; j < V; ++j) {
+                float v0 = h0.v[j] - courant * (dy[2].v[j] - dz[1].v[j]);
+                float v1 = h1.v[j] - courant * (dz[0].v[j] - dx[2].v[j]);
+                float v2 = h2.v[j] - courant * (dx[1].v[j] - dy[0].v[j]);
+                const int gz = zv + j;
+                if (q == a.source_x && wave_ok && gz < nz) {
+                    const i64 sidx = (i64)gy * nz + gz;
+                    const i64 syz = (i64)ny * nz;
+                    v1 = v1 - (a.src_e[2 * syz + sidx] * a.waves_e[2 * a.waves_cols + t]) * courant;
+                    v2 = v2 + (a.src_e[syz + sidx] * a.waves_e[a.waves_cols + t]) * courant;
+                }
+                o[0].v[j] = v0;
+                o[1].v[j] = v1;
+                o[2].v[j] = v2;
+            }
+            float *dst = Hn + (i64)q * plane + g_off;
+            stv<V>(dst, o[0]);
+            stv<V>(dst + cols, o[1]);
+            stv<V>(dst + 2 * cols, o[2]);
+        }
+        __syncthreads();
+        if (k - 1 + S <= last) {
+            if (tid == 0) issue(k - 1 + S);
+            issued = k - 1 + S;
+        }
+    }
+    if (timed_out) {
+        if (tid == 0) {
+            if (a.error) atomicExch(a.error, 1);
+            for (int j = done + 1; j <= issued; ++j)
+                mbar_wait_bounded(bars + (j % S), (j / S) & 1, limit);
+        }
+        __syncthreads();
+    }
+}
+
+static inline size_t up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+static FzLayout fz_layout(int ty, int P, int RZ, int S, int mat) {
+    FzLayout L;
+    L.ty = ty;
+    L.P = P;
+    L.HB = P + 4;
+    L.MB = mat == 1 ? (int)up(P, 16) : P;
+    L.RZ = RZ;
+    L.S = S;
+    size_t hb = (size_t)3 * (ty + 2) * L.HB * 4;
+    size_t eb = (size_t)3 * (ty + 1) * P * 4;
+    size_t mb = (size_t)(ty + 1) * L.MB * (mat == 1 ? 1 : 4);
+    size_t zeb = (size_t)2 * (ty + 1) * RZ * 4;
+    size_t zhb = (size_t)2 * ty * RZ * 4;
+    L.off_h = 0;
+    L.off_e = (int)up(hb, 128);
+    L.off_m = (int)(L.off_e + up(eb, 128));
+    L.off_pze = (int)(L.off_m + up(mb, 128));
+    L.off_pzh = (int)(L.off_pze + up(zeb, 128));
+    L.stage_bytes = (int)(L.off_pzh + up(zhb, 128));
+    L.tx_bytes = (unsigned)(hb + eb + mb + (RZ > 0 ? zeb + zhb : 0));
+    L.off_stages = 128;
+    L.RW = P + 4;
+    L.off_ring = (int)(L.off_stages + (size_t)S * L.stage_bytes);
+    size_t ring = (size_t)2 * 3 * (ty + 1) * L.RW * 4;
+    L.off_coef = (int)up(L.off_ring + ring, 16);
+    size_t coef = (size_t)(2 * (ty + 1) + 2 * P) * 16;
+    L.off_mtab = (int)up(L.off_coef + coef, 16);
+    L.smem_bytes = (int)(L.off_mtab + (mat == 1 ? 256 * 4 : 0));
+    return L;
+}
+
+bool fz_eligible(const fdtd_step_args &a) {
+    if (a.packed != FDTD_PSI_SLAB) return false;
+    if (a.pitch_z % 4 != 0 || a.pitch_z > 248) return false;
+    if (a.material_kind == 1 && a.material_pitch % 16 != 0) return false;
+    if (a.psi_rz % 4 != 0) return false;
+    auto al16 = [](const void *p) { return ((uintptr_t)p & 15) == 0; };
+    for (int j = 0; j < 2; ++j)
+        if (!al16(a.E[j]) || !al16(a.H[j]) || !al16(a.psi_e[j]) || !al16(a.psi_h[j])) return false;
+    return a.material_kind == 1 ? al16(a.material) : al16(a.inv_eps);
+}
+
+int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
+    int rc = get_encoder();
+    if (rc) return rc;
+    const int P = a.pitch_z, ty = a.tile_y, RZ = a.psi_rz;
+    int S = a.stages > 0 ? a.stages : 3;
+    if (S < 2 || S > 4) {
+        set_error("fdtd_step_fused: full-z path takes 2..4 stages");
+        return FDTD_ERR_ARG;
+    }
+    FzLayout L = fz_layout(ty, P, RZ, S, a.material_kind);
+    while (L.smem_bytes > 220 * 1024 && S > 2) L = fz_layout(ty, P, RZ, --S, a.material_kind);
+    const int V = a.vector == 2 ? 2 : 4;
+    const int lanes = P / V;
+    if (L.smem_bytes > 220 * 1024 || lanes * (ty + 1) > 512 || ty + 2 > 256) {
+        set_error("fdtd_step_fused: full-z tile of %d rows does not fit (%d bytes, %d threads)", ty,
+                  L.smem_bytes, lanes * (ty + 1));
+        return FDTD_ERR_ARG;
+    }
+    FzMaps maps;
+    const cuuint64_t nz = a.nz, ny = a.ny, nx = a.nx, pz = P;
+    cuuint64_t fdims[4] = {nz, ny, nx, 3};
+    cuuint64_t fstr[3] = {pz * 4, pz * ny * 4, pz * ny * nx * 4};
+    cuuint32_t hbox[4] = {(cuuint32_t)L.HB, (cuuint32_t)(ty + 2), 1, 3};
+    cuuint32_t ebox[4] = {(cuuint32_t)P, (cuuint32_t)(ty + 1), 1, 3};
+    for (int j = 0; j < 2; ++j) {
+        if ((rc = encode(&maps.H[j], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.H[j], fdims, fstr, hbox)))
+            return rc;
+        if ((rc = encode(&maps.E[j], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.E[j], fdims, fstr, ebox)))
+            return rc;
+    }
+    if (a.material_kind == 1) {
+        const cuuint64_t mp = a.material_pitch;
+        cuuint64_t mdims[3] = {nz, ny, nx};
+        cuuint64_t mstr[2] = {mp, mp * ny};
+        cuuint32_t mbox[3] = {(cuuint32_t)L.MB, (cuuint32_t)(ty + 1), 1};
+        if ((rc = encode(&maps.M, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, a.material, mdims, mstr, mbox)))
+            return rc;
+    } else {
+        cuuint64_t mdims[3] = {nz, ny, nx};
+        cuuint64_t mstr[2] = {pz * 4, pz * ny * 4};
+        cuuint32_t mbox[3] = {(cuuint32_t)L.MB, (cuuint32_t)(ty + 1), 1};
+        if ((rc = encode(&maps.M, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, a.inv_eps, mdims, mstr, mbox)))
+            return rc;
+    }
+    FzParams prm;
+    prm.a = a;
+    prm.L = L;
+    prm.xoff = 0;
+    prm.yoff = (long long)2 * a.psi_rx * a.ny * P;
+    prm.zoff = prm.yoff + (long long)2 * a.psi_ry * a.nx * P;
+    if (RZ > 0) {
+        const cuuint64_t rz = RZ;
+        cuuint64_t zdims[4] = {rz, ny, nx, 2};
+        cuuint64_t zstr[3] = {rz * 4, rz * ny * 4, rz * ny * nx * 4};
+        cuuint32_t zebox[4] = {(cuuint32_t)RZ, (cuuint32_t)(ty + 1), 1, 2};
+        cuuint32_t zhbox[4] = {(cuuint32_t)RZ, (cuuint32_t)ty, 1, 2};
+        for (int j = 0; j < 2; ++j) {
+            if ((rc = encode(&maps.PZE[j], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.psi_e[j] + prm.zoff,
+                             zdims, zstr, zebox)))
+                return rc;
+            if ((rc = encode(&maps.PZH[j], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.psi_h[j] + prm.zoff,
+                             zdims, zstr, zhbox)))
+                return rc;
+        }
+    } else {
+        maps.PZE[0] = maps.PZE[1] = maps.PZH[0] = maps.PZH[1] = maps.M;  // never loaded
+    }
+    const int tiles = (a.ny + ty - 1) / ty;
+    const int chunks = (a.nx + a.chunk_x - 1) / a.chunk_x;
+    dim3 grid((unsigned)(tiles * chunks));
+    dim3 threads((unsigned)lanes, (unsigned)(ty + 1));
+#define LAUNCH3(M, SS, W)                                                                    \
+    do {                                                                                     \
+        cudaFuncSetAttribute(fz_step_kernel<M, SS, W>,                                       \
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem_bytes);      \
+        fz_step_kernel<M, SS, W><<<grid, threads, L.smem_bytes, stream>>>(maps, prm);        \
+    } while (0)
+#define LAUNCH(M, SS)                                                                        \
+    do {                                                                                     \
+        if (V == 4) LAUNCH3(M, SS, 4); else LAUNCH3(M, SS, 2);                                \
+    } while (0)
+    if (a.material_kind == 1) {
+        if (S == 2) LAUNCH(1, 2); else if (S == 3) LAUNCH(1, 3); else LAUNCH(1, 4);
+    } else {
+        if (S == 2) LAUNCH(0, 2); else if (S == 3) LAUNCH(0, 3); else LAUNCH(0, 4);
+    }
+#undef LAUNCH3
+#undef LAUNCH
+    return launch_status("fdtd_step_fused (full-z TMA)");
+}
+
+}  // namespace wfb

@@ -15,11 +15,13 @@ struct TmaLayout {
     int off_e, off_m;      // byte offsets of the E and material boxes in a stage
     int stage_bytes;       // bytes per stage (128-byte aligned pieces)
     unsigned tx_bytes;     // bytes the three TMA loads of a stage deliver
-    int off_stages, off_enew, off_mtab, smem_bytes;
+    int off_stages, off_enew, off_coef, off_mtab, smem_bytes;
 };
 
 TmaLayout tma_layout(int ty, int tz, int stages, int mat);
 bool tma_eligible(const fdtd_step_args &a);
 int launch_tma(const fdtd_step_args &a, cudaStream_t stream);
+bool fz_eligible(const fdtd_step_args &a);
+int launch_fz(const fdtd_step_args &a, cudaStream_t stream);
 
 }  // namespace wfb

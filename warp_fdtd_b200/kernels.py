@@ -111,3 +111,28 @@ def _retreat(step, stream=None):
 # kernels.py:151-153 and adjoint.py:226-228
 advance = Kernel("advance", _advance, lambda *a: 1)
 retreat = Kernel("retreat", _retreat, lambda *a: 1)
+
+
+def pack_index(full, coeff4, shape):
+    """Gather a (6, n) by-cell CPML state into the reference's packed layout
+    (kernels.py:50-74 index formula) given the (3, L, 4) ranked table."""
+    nx, ny, nz = shape
+    c = coeff4.detach().cpu()
+    sizes = []
+    for axis, length in enumerate(shape):
+        sizes.append(int((c[axis, :length, 0] != 0).sum()) * (nx * ny * nz // length))
+    out = torch.zeros((6, max(1, *sizes)), dtype=full.dtype, device=full.device)
+    f = full.view(6, nx, ny, nz)
+    for axis, length in enumerate(shape):
+        for pos in range(length):
+            if float(c[axis, pos, 0]) == 0.0:
+                continue
+            r = int(c[axis, pos, 3])
+            for slot in (2 * axis, 2 * axis + 1):
+                if axis == 0:
+                    out[slot, r * ny * nz:(r + 1) * ny * nz] = f[slot, pos].reshape(-1)
+                elif axis == 1:
+                    out[slot, r * nx * nz:(r + 1) * nx * nz] = f[slot, :, pos].reshape(-1)
+                else:
+                    out[slot, r * nx * ny:(r + 1) * nx * ny] = f[slot, :, :, pos].reshape(-1)
+    return out

@@ -152,7 +152,9 @@ class Solver:
             raise ValueError("graph_steps must be positive")
         self.courant = factor / np.sqrt(3)
         self.tile = tuple(tile) if tile else (0, 0, 0)
-        self.path = int(path)
+        if path not in (0, 1, 2, 3):
+            raise ValueError("path must be 0 (auto), 1, 2 or 3")
+        self.kernel_path = int(path)
         dev = self.device
         f32 = dict(dtype=torch.float32, device=dev)
         nx, ny, nz = self.shape
@@ -191,17 +193,32 @@ class Solver:
         self.coeffs, self._coeff4 = {}, {}
         tables = {f: cpml_coefficients(m, d, self.shape, f) for f in "EH"}
         packed = {f: pack_coefficients(tables[f], self.shape) for f in "EH"}
-        # one column count serves both fields' psi arrays (the fused kernel
-        # addresses E and H state with the same stride)
-        self._psi_cols = (max(packed["E"][1], packed["H"][1]) if cpml_storage == "packed"
-                          else self._cells)
         for field in "EH":
-            packed4 = packed[field][0]
-            table = packed4 if cpml_storage == "packed" else tables[field]
+            table = packed[field][0] if cpml_storage == "packed" else tables[field]
             self.coeffs[field] = torch.from_numpy(table).to(dev)
-            self._coeff4[field] = torch.from_numpy(packed4).to(dev)
-            setattr(self, "_psi_" + field.lower(),
-                    [torch.zeros((6, self._psi_cols), **f32) for _ in range(2)])
+            self._coeff4[field] = torch.from_numpy(packed[field][0]).to(dev)
+        # CPML state layout: the full-z pipeline (path 3, default when rows fit
+        # one TMA box) keeps psi in slab blocks (x, y, z-rank); the other paths
+        # use the reference's full or packed layout.
+        use_slab = self.kernel_path in (0, 3) and self._pitch <= 248
+        if self.kernel_path == 3 and not use_slab:
+            raise ValueError("path 3 needs nz <= 248")
+        active = [max(int((packed[f][0][axis, :self.shape[axis], 0] != 0).sum()) for f in "EH")
+                  for axis in range(3)]
+        self._psi_r = (active[0], active[1], (active[2] + 3) // 4 * 4)
+        if use_slab:
+            self._psi_layout = 2
+            rx, ry, rz = self._psi_r
+            self._psi_cols = max(1, 2 * rx * ny * self._pitch + 2 * ry * nx * self._pitch
+                                 + 2 * nx * ny * rz)
+            shape = (self._psi_cols,)
+        else:
+            self._psi_layout = 1 if cpml_storage == "packed" else 0
+            self._psi_cols = (max(packed["E"][1], packed["H"][1]) if cpml_storage == "packed"
+                              else self._cells)
+            shape = (6, self._psi_cols)
+        for field in "EH":
+            setattr(self, "_psi_" + field.lower(), [torch.zeros(shape, **f32) for _ in range(2)])
 
         # plane mode source (solver.py:132-182)
         sources = [o for o in m["objects"] if o["class"] == "ModePlaneSource"]
@@ -275,15 +292,48 @@ class Solver:
         """H(n-1/2) after the last issued step (zeros before the first)."""
         return self._compact(self._H[(self._issued + 1) & 1], 3)
 
+    def _psi_reference(self, buf, field):
+        """CPML state in the reference layout: (6, n) by cell for
+        cpml_storage="full", (6, packed size) by plane rank for "packed"
+        (solver.py:124-131).  Inactive entries are zero."""
+        if self._psi_layout == 1:
+            return buf
+        if self._psi_layout == 0:
+            return self._compact(buf, 6)
+        nx, ny, nz = self.shape
+        P = self._pitch
+        rx, ry, rz = self._psi_r
+        c4 = self._coeff4[field].cpu()
+        full = torch.zeros((6, nx, ny, nz), dtype=torch.float32, device=self.device)
+        xb = buf[: 2 * rx * ny * P].view(2, rx, ny, P)
+        yb = buf[2 * rx * ny * P: 2 * rx * ny * P + 2 * ry * nx * P].view(2, ry, nx, P)
+        zb = buf[2 * rx * ny * P + 2 * ry * nx * P:][: 2 * nx * ny * rz].view(2, nx, ny, rz)
+        for x in range(nx):
+            if float(c4[0, x, 0]) != 0.0:
+                r = int(c4[0, x, 3])
+                full[0:2, x] = xb[:, r, :, :nz]
+        for y in range(ny):
+            if float(c4[1, y, 0]) != 0.0:
+                r = int(c4[1, y, 3])
+                full[2:4, :, y] = yb[:, r, :, :nz]
+        for z in range(nz):
+            if float(c4[2, z, 0]) != 0.0:
+                r = int(c4[2, z, 3])
+                full[4:6, :, :, z] = zb[:, :, :, r]
+        full = full.reshape(6, self.n)
+        if self.cpml_storage == "packed":
+            from .kernels import pack_index
+
+            return pack_index(full, self._coeff4[field], self.shape)
+        return full
+
     @property
     def psi_e(self):
-        buf = self._psi_e[self._issued & 1]
-        return buf if self.cpml_storage == "packed" else self._compact(buf, 6)
+        return self._psi_reference(self._psi_e[self._issued & 1], "E")
 
     @property
     def psi_h(self):
-        buf = self._psi_h[self._issued & 1]
-        return buf if self.cpml_storage == "packed" else self._compact(buf, 6)
+        return self._psi_reference(self._psi_h[self._issued & 1], "H")
 
     def _sync_eps(self):
         """Copy `eps` (n,) into the padded float32 material the kernel reads."""
@@ -298,10 +348,11 @@ class Solver:
             a.psi_e[j] = ptr(self._psi_e[j])
             a.psi_h[j] = ptr(self._psi_h[j])
         a.psi_cols = self._psi_cols
+        a.psi_rx, a.psi_ry, a.psi_rz = self._psi_r
         a.coeff_e = ptr(self._coeff4["E"])
         a.coeff_h = ptr(self._coeff4["H"])
         a.clen = int(self._coeff4["E"].shape[1])
-        a.packed = int(self.cpml_storage == "packed")
+        a.packed = int(self._psi_layout)
         a.material_kind = self.material_kind
         if self.material_kind == 0:
             a.inv_eps = ptr(self._eps_p)
@@ -321,7 +372,7 @@ class Solver:
         a.pitch_z = self._pitch
         a.material_pitch = self._mpitch
         a.tile_y, a.tile_z, a.chunk_x = (int(v) for v in self.tile)
-        a.path = int(self.path)
+        a.path = int(self.kernel_path)
         return a
 
     def set_tile(self, tile_y, tile_z, chunk_x=0):
@@ -330,11 +381,6 @@ class Solver:
         self._args = self._step_args()
         self.graphs = {}
 
-    def set_path(self, path):
-        """0 auto, 1 shared-memory staging, 2 TMA pipeline; drops captured graphs."""
-        self.path = int(path)
-        self._args = self._step_args()
-        self.graphs = {}
 
     def refresh_material(self):
         """Propagate an in-place change of `eps` to the copy the fused kernel reads."""
