@@ -1,0 +1,380 @@
+"""Benchmark: the 20 nm silicon bend forward (324 x 324 x 144 cells, 4000 steps).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One bench step is one complete forward trajectory of the bend workload
+(reset + 4000 fused Yee steps + the two 5-wavelength modal detectors), i.e.
+6.05e10 cell-updates.  The metric is Gcell-updates/s over the whole job.
+Under torchrun (N > 1) every rank runs its own independent replica of the
+workload on its GPU (the path does not shard; there is no collective in the
+data path) and `value` is the sum over ranks of cell-updates divided by the
+maximum over ranks of the device time.
+
+Printed on rank 0: one JSON line with the contract's keys plus `roofline`
+(the fused step kernel against the measured HBM copy bandwidth, 49 algorithmic
+bytes per cell-update), `cpu_baseline` (the CPU oracle on this host's cores on
+a bounded sample of the same grid), `e2e` (the same metric through the public
+Solver API with the material grid uploaded from pinned host memory and the
+detector phasors read back every step), `clocks` and `gpu_launches`.
+
+`--impl reference` times the reference's CPU path on this host: warp-lang
+(the reference's runtime) is not installable here, so the arm runs the CPU
+restatement of the reference kernels (oracle/, C + OpenMP, all host threads)
+on a bounded sample of the same workload per step.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOADS = {
+    # name: (interior_um, time_steps)
+    "bend20": ((6.0, 6.0, 2.4), 4000),
+    # profiling case of the same kernel: 174 x 174 x 144 cells (fields 4 x 70 MB > L2)
+    "bend20-small": ((3.0, 3.0, 2.4), 200),
+}
+WORKLOAD = "bend20nm_324x324x144_4000steps_5lambda"
+METRIC = "Gcell-updates/s (20 nm bend forward)"
+BYTES_PER_CELL = 49  # read E, H (24 B) + write E, H (24 B) + 1 B material index
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def bundle_dir(workload="bend20", time_steps=None):
+    base = Path(os.environ.get("FDTD_BENCH_CACHE", tempfile.gettempdir())) / "warp_fdtd_b200_bench"
+    interior, steps = WORKLOADS[workload]
+    return base / f"{workload}_{time_steps or steps}"
+
+
+def make_bundle(workload="bend20", time_steps=None):
+    from warp_fdtd_b200 import scene
+
+    interior, steps = WORKLOADS[workload]
+    d = bundle_dir(workload, time_steps)
+    if not (d / "manifest.json").exists():
+        d.parent.mkdir(parents=True, exist_ok=True)
+        tmp = d.with_name(d.name + f".tmp{os.getpid()}")
+        scene.bend_case(tmp, interior_um=interior, steps=time_steps or steps)
+        try:
+            os.replace(tmp, d)
+        except OSError:
+            pass  # another rank won the race
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def reduce_max(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def cpu_sample(case, time_steps, threads=None):
+    """The CPU oracle's fused update on the full grid for `time_steps` steps."""
+    from oracle import cpu as ocpu
+    from oracle.model import OracleSolver
+
+    o = OracleSolver(case)
+    L = ocpu.lib()
+    nx, ny, nz = o.shape
+    start = time.perf_counter()
+    L.oracle_run_steps(o.E, o.H, o.eps, o.psi_e, o.psi_h, o.coeffs["E"], o.coeffs["H"],
+                       o.coeffs["E"].shape[1], o.sources["E"], o.sources["H"], o.waves["E"],
+                       o.waves["H"], o.steps, 0, time_steps, nx, ny, nz, int(o.source_x),
+                       float(o.courant))
+    sec = time.perf_counter() - start
+    return o.n * time_steps / sec / 1e9, ocpu.num_threads(), sec
+
+
+def run_reference(args, world, rank):
+    """Reference arm: the CPU restatement of the reference kernels (oracle)."""
+    if rank != 0:
+        return
+    case = make_bundle(args.workload, args.time_steps)
+    sample_steps = int(os.environ.get("FDTD_REF_SAMPLE_STEPS", "20"))
+    for _ in range(args.warmup):
+        cpu_sample(case, sample_steps)
+    rates, secs, cores = [], [], 1
+    for _ in range(args.steps):
+        r, cores, s = cpu_sample(case, sample_steps)
+        rates.append(r)
+        secs.append(s)
+    value = statistics.median(rates)
+    sample = (f"{sample_steps} of 4000 time steps on the full 324x324x144 grid per step, "
+              "E+H updates with CPML and source (oracle/fdtd_oracle.c, OpenMP)")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Gcell-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * statistics.median(secs), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "grid": [324, 324, 144], "time_steps": 4000,
+                   "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "Gcell-updates/s", "cores": cores,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "warp-lang is not installed here; the reference's CPU path is timed as its "
+                "C restatement",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from warp_fdtd_b200 import _lib
+    from warp_fdtd_b200.detectors import attach, measurements
+    from warp_fdtd_b200.solver import Solver
+
+    case = make_bundle(args.workload, args.time_steps)
+    s = Solver(case, graph_steps=64)
+    attach(s)
+    s.compile()
+    stream = torch.cuda.current_stream()
+    cells = s.n * s.steps
+
+    for _ in range(args.warmup):
+        s.reset()
+        s.run()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        s.reset()
+        s.run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clock_info = clocks.stop()
+    ms_local = e0.elapsed_time(e1)
+    ms = reduce_max(ms_local, world)
+    total_cells = reduce_sum(float(cells * args.steps), world)
+    value = total_cells / (ms / 1e3) / 1e9
+    meas = measurements(s)
+    launches_per_step = 1 + sum(1 for m in s.monitors if m.shared is None) + 1
+
+    # dominant kernel alone: average duration of the fused step over 200 launches
+    s.reset()
+    for _ in range(5):
+        _lib.call("fdtd_step_fused", s._args, stream.cuda_stream)
+    k0 = torch.cuda.Event(enable_timing=True)
+    k1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    k0.record(stream)
+    nk = 200
+    for _ in range(nk):
+        _lib.call("fdtd_step_fused", s._args, stream.cuda_stream)
+    k1.record(stream)
+    torch.cuda.synchronize()
+    kernel_ms = k0.elapsed_time(k1) / nk
+    achieved = BYTES_PER_CELL * s.n / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = load_peaks()
+    traffic = None
+    tfile = ROOT / "profiles" / "fused_step_traffic.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get("bytes_per_launch")
+        except (ValueError, OSError):
+            traffic = None
+
+    # end to end through the public API: material upload from pinned host memory,
+    # full trajectory, phasor read-back and the host modal overlap, every step
+    host_mat = torch.empty(s.material.numel(), dtype=torch.uint8, pin_memory=True)
+    host_mat.copy_(s.material.cpu())
+    phasor_bytes = sum(m.phasor.numel() * 8 for m in s.monitors if m.shared is None)
+    e2e_steps = max(1, min(args.steps, 3))
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.material.copy_(host_mat, non_blocking=True)
+        s.reset()
+        s.run()
+        meas = measurements(s)
+    torch.cuda.synchronize()
+    e2e_sec = reduce_max(time.perf_counter() - t0, world)
+    e2e_value = reduce_sum(float(cells * e2e_steps), world) / e2e_sec / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        sample_steps = int(os.environ.get("FDTD_CPU_SAMPLE_STEPS", "60"))
+        rate, cores, sec = cpu_sample(case, sample_steps)
+        cpu = {"value": rate, "unit": "Gcell-updates/s", "cores": cores, "kind": "port",
+               "sample": f"{sample_steps} of 4000 time steps on the full 324x324x144 grid "
+                         f"({sec:.1f} s), CPU oracle E+H updates with CPML and source"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD if args.workload == "bend20" and s.steps == 4000
+                       else f"{args.workload}_{list(s.shape)}_{s.steps}steps",
+                       "grid": list(s.shape), "time_steps": s.steps,
+                       "cells": s.n, "materials": "uint8 index (SiO2 2.085, Si 12.11)",
+                       "detectors": "mode_in, mode_out x 5 wavelengths (float64 DFT)",
+                       "l2": "inputs larger than L2 (fields 4 x 181 MB ping-pong)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "fz_step_kernel (fdtd_step_fused, path 3)",
+                         "kernel_ms": kernel_ms, "bytes_per_cell": BYTES_PER_CELL,
+                         "peak_kind": f"{peak_kind} (copy bandwidth)"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "Gcell-updates/s",
+                    "h2d_bytes_per_step": int(host_mat.numel()),
+                    "d2h_bytes_per_step": int(phasor_bytes)},
+            "gpu_launches": int(launches_per_step * s.steps * args.steps),
+            "clocks": clock_info,
+            "modal_transmission_1550nm": meas.get("modal_transmission_spectrum", [None] * 3)[2],
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline sample")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="bend20",
+                    help="bend20 is the benchmark; bend20-small is for profiling captures")
+    ap.add_argument("--time-steps", type=int, default=None,
+                    help="override the trajectory length (profiling only)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, world, rank)
+        return
+    world, rank, local = dist_setup()
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
