@@ -222,6 +222,28 @@ int fdtd_record_flux64(const float *E0, const float *E1, const float *H0, const 
                        int y0, int z0, int sx, int sy, int sz, int axis, int exact,
                        void *stream);
 
+/* Batched form of fdtd_record_phasor64 for CUDA-graph step loops: each step
+ * writes the six colocated (or raw) float32 samples of the plane into slot
+ * t % T of `stage` ((T, 6, count) float32, count = sx*sy*sz), skipping steps
+ * with t >= nsteps or indices[t] < 0; fdtd_dft_fold then adds the staged
+ * steps to the float64 phasors.  Same buffer convention as
+ * fdtd_record_phasor64. */
+int fdtd_record_stage(const float *E0, const float *E1, const float *H0, const float *H1,
+                      const int *step, const int *indices, int nsteps, float *stage, int T,
+                      int nx, int ny, int nz, int pitch_z, int x0, int y0, int z0, int sx,
+                      int sy, int sz, int exact, void *stream);
+
+/* Fold the steps staged since the last fold into the phasors, in time order:
+ * run after fdtd_advance once every T steps and after the last step.  With
+ * s = step[0] (steps completed) the window is [T * floor((s - 1) / T), s).
+ * For each step t of the window with indices[t] >= 0 and each frequency k
+ * with w = weights[k, t] != 0: phasor[k, c, i] += w * stage[t % T, c, i]
+ * (float64, the same operation sequence as fdtd_record_phasor64, so the
+ * result is bitwise identical). */
+int fdtd_dft_fold(const int *step, const int *indices, int nsteps, const float *weights,
+                  int nfreq, const float *stage, int T, double *phasor, long long count,
+                  void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,3 +85,30 @@ def test_graph_replay_and_tiles_identical(tmp_path):
             np.testing.assert_array_equal(f["E"], ref[0]["E"])
             np.testing.assert_array_equal(f["H"], ref[0]["H"])
             np.testing.assert_array_equal(ph, ref[1])
+
+
+def test_batched_dft_mid_trajectory_reads(tmp_path):
+    """Phasors read between batch boundaries include the pending steps (folded
+    into a copy) and later folds do not count them twice."""
+    from oracle.model import OracleSolver
+    from warp_fdtd_b200.solver import Solver
+    from warp_fdtd_b200.detectors import attach
+
+    case = make_bundle(tmp_path / "b", (12, 14, 40), 75, seed=12)
+    o = OracleSolver(case).attach()
+    s = Solver(case, graph_steps=64)
+    attach(s)
+    s.reset()
+    mode = {m.name: m for m in s.monitors}["mode_in"]
+    omode = {m.name: m for m in o.monitors}["mode_in"]
+    for n in (20, 45):  # 20 < batch 32, 45 straddles the fold at 32
+        while s._issued < n:
+            s.launch_step()
+        o.run(n - int(o.step[0]))
+        got = mode.phasors()
+        want = (omode.phasor[0][..., 0] + 1j * omode.phasor[0][..., 1]).reshape(6, *omode.shape)
+        np.testing.assert_array_equal(got, want)
+    while s._issued < s.steps:
+        s.launch_step()
+    o.run(s.steps - int(o.step[0]))
+    np.testing.assert_array_equal(mode.phasor.cpu().numpy(), omode.phasor)

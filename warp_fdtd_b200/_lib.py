@@ -85,6 +85,9 @@ _SIGNATURES = {
     "fdtd_step_fused": [ctypes.POINTER(StepArgs), _p],
     "fdtd_record_phasor64": [_p, _p, _p, _p, _p, _p, _i, _p, _i, _p, _i, _i, _i, _i, _i, _i,
                              _i, _i, _i, _i, _i, _p],
+    "fdtd_record_stage": [_p, _p, _p, _p, _p, _p, _i, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i,
+                          _i, _i, _i, _p],
+    "fdtd_dft_fold": [_p, _p, _i, _p, _i, _p, _i, _p, _ll, _p],
     "fdtd_record_flux64": [_p, _p, _p, _p, _p, _p, _i, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i,
                            _i, _i, _i, _i, _i, _p],
 }

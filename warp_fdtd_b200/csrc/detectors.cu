@@ -88,6 +88,78 @@ __global__ void record_flux64_kernel(const float *__restrict__ E0, const float *
     }
 }
 
+__global__ void record_stage_kernel(const float *__restrict__ E0, const float *__restrict__ E1,
+                                    const float *__restrict__ H0, const float *__restrict__ H1,
+                                    const int *__restrict__ step,
+                                    const int *__restrict__ indices, int nsteps,
+                                    float *__restrict__ stage, int T, int nx, int ny, int nz,
+                                    int pitch, int x0, int y0, int z0, int sx, int sy, int sz,
+                                    int exact) {
+    const i64 count = (i64)sx * sy * sz;
+    i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int t = step[0];
+    if (t < 0 || t >= nsteps || indices[t] < 0) return;
+    const int s = t & 1;
+    const float *e = s ? E0 : E1;
+    const float *h = s ? H0 : H1;
+    const float *prev = s ? H1 : H0;
+    const i64 n = (i64)nx * ny * pitch;
+    int x = x0 + (int)(i / ((i64)sy * sz));
+    int y = y0 + (int)((i / sz) % sy);
+    int z = z0 + (int)(i % sz);
+    float ee[3], hh[3];
+    plane_sample(e, h, prev, n, x, y, z, nx, ny, nz, exact, ee, hh, pitch);
+    float *dst = stage + (i64)(t % T) * 6 * count + i;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        dst[(i64)c * count] = ee[c];
+        dst[(i64)(c + 3) * count] = hh[c];
+    }
+}
+
+// One thread per (component, cell); the window's weights are staged in
+// shared memory ([k][t] float2).
+__global__ void dft_fold_kernel(const int *__restrict__ step, const int *__restrict__ indices,
+                                int nsteps, const float2 *__restrict__ weights, int nfreq,
+                                const float *__restrict__ stage, int T,
+                                double2 *__restrict__ phasor, i64 count) {
+    extern __shared__ float2 wsm[];  // [nfreq][T]
+    __shared__ int valid[256];
+    const int s = step[0];
+    if (s <= 0) return;
+    const int t0 = ((s - 1) / T) * T;
+    const int n = s - t0;
+    for (int j = threadIdx.x; j < nfreq * T; j += blockDim.x) {
+        const int k = j / T, dt = j - k * T;
+        const int t = t0 + dt;
+        wsm[j] = (dt < n && t < nsteps) ? weights[(i64)k * nsteps + t] : make_float2(0.f, 0.f);
+    }
+    for (int j = threadIdx.x; j < T; j += blockDim.x) {
+        const int t = t0 + j;
+        valid[j] = (j < n && t < nsteps && indices[t] >= 0) ? 1 : 0;
+    }
+    __syncthreads();
+    const i64 gid = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= 6 * count) return;
+    const int c = (int)(gid / count);
+    const i64 i = gid - (i64)c * count;
+    for (int k = 0; k < nfreq; ++k) {
+        double2 *p = phasor + ((i64)k * 6 + c) * count + i;
+        double2 acc = *p;
+        for (int dt = 0; dt < n; ++dt) {
+            if (!valid[dt]) continue;
+            const float2 w = wsm[k * T + dt];
+            const double wr = w.x, wi = w.y;
+            if (wr == 0.0 && wi == 0.0) continue;
+            const double v = (double)stage[((i64)((t0 + dt) % T) * 6 + c) * count + i];
+            acc.x = acc.x + wr * v;
+            acc.y = acc.y + wi * v;
+        }
+        *p = acc;
+    }
+}
+
 }  // namespace wfb
 
 using namespace wfb;
@@ -132,6 +204,40 @@ int fdtd_record_flux64(const float *E0, const float *E1, const float *H0, const 
         E0, E1, H0, H1, step, indices, nsteps, area, flux, nbins, nx, ny, nz, pitch_z, x0, y0,
         z0, sx, sy, sz, axis, exact);
     return launch_status("fdtd_record_flux64");
+}
+
+int fdtd_record_stage(const float *E0, const float *E1, const float *H0, const float *H1,
+                      const int *step, const int *indices, int nsteps, float *stage, int T,
+                      int nx, int ny, int nz, int pitch_z, int x0, int y0, int z0, int sx,
+                      int sy, int sz, int exact, void *stream) {
+    const i64 count = (i64)sx * sy * sz;
+    if (pitch_z <= 0) pitch_z = nz;
+    if (count <= 0 || T < 1 || T > 256 || nsteps < 1 || pitch_z < nz || !E0 || !E1 || !H0 ||
+        !H1 || !step || !indices || !stage || x0 < 0 || y0 < 0 || z0 < 0 || x0 + sx > nx ||
+        y0 + sy > ny || z0 + sz > nz) {
+        set_error("fdtd_record_stage: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    record_stage_kernel<<<(unsigned)((count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        E0, E1, H0, H1, step, indices, nsteps, stage, T, nx, ny, nz, pitch_z, x0, y0, z0, sx, sy,
+        sz, exact);
+    return launch_status("fdtd_record_stage");
+}
+
+int fdtd_dft_fold(const int *step, const int *indices, int nsteps, const float *weights,
+                  int nfreq, const float *stage, int T, double *phasor, long long count,
+                  void *stream) {
+    if (!step || !indices || !weights || !stage || !phasor || nfreq < 1 || nfreq > 64 ||
+        T < 1 || T > 256 || nfreq * T > 6144 || count < 1 || nsteps < 1) {
+        set_error("fdtd_dft_fold: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    const i64 work = 6 * (i64)count;
+    const size_t smem = (size_t)nfreq * T * sizeof(float2);
+    dft_fold_kernel<<<(unsigned)((work + 255) / 256), 256, smem, (cudaStream_t)stream>>>(
+        step, indices, nsteps, (const float2 *)weights, nfreq, stage, T, (double2 *)phasor,
+        count);
+    return launch_status("fdtd_dft_fold");
 }
 
 }  // extern "C"

@@ -100,6 +100,13 @@ class Monitor:
         self.area = torch.from_numpy(
             np.ascontiguousarray(self.area_numpy.ravel(), np.float32)).to(dev)
         self.shared = None  # monitor whose accumulator this one aliases
+        self._solver = solver
+        # Phasor DFTs are batched: each step stages the float32 samples, a fold
+        # every `batch` steps adds them to the float64 phasors in time order.
+        self.batch = int(np.gcd(int(solver.graph_steps), 32)) if self.is_phasor else 1
+        self.stage = (torch.zeros((self.batch, 6, self.n), dtype=torch.float32, device=dev)
+                      if self.is_phasor else None)
+        self._folded = 0  # steps already folded (host mirror)
 
     def _key(self):
         return (tuple(map(tuple, self.obj["grid_slice"])), self.exact, self.is_phasor,
@@ -109,6 +116,21 @@ class Monitor:
         if self.shared is None:
             self.phasor.zero_()
             self.flux.zero_()
+        self._folded = 0
+
+    def fold(self, s, issued, into=None):
+        """Add the steps staged since the last batch boundary to the phasors
+        (the window comes from the device step counter).  Folds happen at
+        every multiple of `batch` steps and after the last step; `into`
+        receives a partial window instead (see phasors)."""
+        if self.shared is not None or not self.is_phasor:
+            return
+        _lib.call("fdtd_dft_fold", ptr(s.step), ptr(self.indices), int(self.indices.numel()),
+                  ptr(self.weights), int(self.weights.shape[0]), ptr(self.stage), self.batch,
+                  ptr(self.phasor if into is None else into), self.n,
+                  _lib.stream_handle(s.device))
+        if into is None:
+            self._folded = issued
 
     def launch(self, s):
         if self.shared is not None:
@@ -119,9 +141,9 @@ class Monitor:
         steps = int(self.indices.numel())
         if self.is_phasor:
             _lib.call(
-                "fdtd_record_phasor64", *common, ptr(self.indices), steps, ptr(self.weights),
-                int(self.weights.shape[0]), ptr(self.phasor), nx, ny, nz, s._pitch, *self.lo,
-                *self.shape, int(self.exact), stream,
+                "fdtd_record_stage", *common, ptr(self.indices), steps, ptr(self.stage),
+                self.batch, nx, ny, nz, s._pitch, *self.lo, *self.shape, int(self.exact),
+                stream,
             )
         else:
             _lib.call(
@@ -131,7 +153,13 @@ class Monitor:
             )
 
     def phasors(self, k=0):
-        raw = self.phasor[k].cpu().numpy()
+        owner = self.shared or self
+        acc = owner.phasor
+        if owner.is_phasor and owner._folded < self._solver._issued:
+            # mid-batch read: add the pending steps to a copy
+            acc = owner.phasor.clone()
+            owner.fold(self._solver, self._solver._issued, into=acc)
+        raw = acc[k].cpu().numpy()
         return (raw[..., 0] + 1j * raw[..., 1]).reshape(6, *self.shape)
 
     def power(self, s, k=0):

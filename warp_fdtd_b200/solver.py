@@ -408,6 +408,10 @@ class Solver:
             monitor.launch(self)
         _lib.call("fdtd_advance", ptr(self.step), 1, stream)
         self._issued += 1
+        for monitor in self.monitors:
+            if monitor.is_phasor and (self._issued % monitor.batch == 0
+                                      or self._issued == self.steps):
+                monitor.fold(self, self._issued)
 
     def compile(self):
         start = time.perf_counter()
@@ -416,11 +420,18 @@ class Solver:
             torch.cuda.synchronize(self.device)
             self.reset()
             for length in {self.graph_steps, self.steps % self.graph_steps} - {0}:
+                # capture at the step offset where the graph will be replayed so
+                # the detectors' folds land on the right steps: full graphs start
+                # on multiples of graph_steps, the tail graph ends the trajectory
+                start = 0 if length == self.graph_steps else self.steps - length
+                self._issued = start
+                for m in self.monitors:
+                    m._folded = start
                 g = torch.cuda.CUDAGraph()
                 with torch.cuda.graph(g, capture_error_mode="relaxed"):
                     for _ in range(length):
                         self.launch_step()
-                self._issued -= length
+                self._issued = 0
                 self.graphs[length] = g
             self.reset()
         return time.perf_counter() - start
@@ -437,6 +448,8 @@ class Solver:
                 if tail:
                     self.graphs[tail].replay()
                 self._issued += self.steps
+                for m in self.monitors:
+                    m._folded = self.steps
             torch.cuda.synchronize(self.device)
 
     def fields(self):
