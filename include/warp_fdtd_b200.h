@@ -129,6 +129,26 @@ int fdtd_material_subpixel_adjoint(const float *rho, const float *g, float *rho_
 int fdtd_material_smooth_adjoint(const float *g, const float *weights, int radius,
                                  float *p_grad, int px, int py, void *stream);
 
+/* record_curl for the fused path's ping-pong buffers (adjoint.py:17-43): with
+ * t = step[0] the H read by step t's E update is H[t & 1] (rows of pitch
+ * pitch_z); hist[hist_step[0], c, j] = courant * curl(H)_c over the design
+ * box; hist is (rows, 3, sx*sy*sz). */
+int fdtd_record_curl_pp(const float *H0, const float *H1, int pitch_z, const int *step,
+                        const int *hist_step, float *hist, int nx, int ny, int nz, int x0,
+                        int y0, int z0, int sx, int sy, int sz, float courant, void *stream);
+
+/* The whole material map of material.py:58-91 in one call: scratch (px*py
+ * floats, caller-owned) receives smooth(p), out receives subpixel(scratch). */
+int fdtd_material_forward(const float *p, const float *weights, int radius, float *scratch,
+                          float *out, int px, int py, float beta, float eps_lo,
+                          float contrast, void *stream);
+
+/* Its pullback (material.py:93-102): p_grad = (d out / d p)^T g, overwritten.
+ * scratch holds 2*px*py floats (the smoothed density and its adjoint). */
+int fdtd_material_backward(const float *p, const float *weights, int radius, const float *g,
+                           float *scratch, float *p_grad, int px, int py, float beta,
+                           float eps_lo, float contrast, void *stream);
+
 /* ---------------------------------------------------------------------------
  * 2. B200 forward path
  * ------------------------------------------------------------------------ */

@@ -74,6 +74,7 @@ _SIGNATURES = {
     "fdtd_record": [_p, _p, _p, _ll, _p, _p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i,
                     _i, _i, _i, _i, _p],
     "fdtd_record_curl": [_p, _ll, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i, _f, _p],
+    "fdtd_record_curl_pp": [_p, _p, _i, _p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i, _f, _p],
     "fdtd_prepare": [_p, _p, _p, _p, _i, _p, _i, _i, _i, _f, _i, _p],
     "fdtd_gather": [_p, _p, _p, _p, _i, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i, _i, _p],
     "fdtd_inject": [_p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i, _i, _p],
@@ -82,6 +83,8 @@ _SIGNATURES = {
     "fdtd_material_smooth_adjoint": [_p, _p, _i, _p, _i, _i, _p],
     "fdtd_material_subpixel": [_p, _p, _i, _i, _f, _f, _f, _p],
     "fdtd_material_subpixel_adjoint": [_p, _p, _p, _i, _i, _f, _f, _f, _p],
+    "fdtd_material_forward": [_p, _p, _i, _p, _p, _i, _i, _f, _f, _f, _p],
+    "fdtd_material_backward": [_p, _p, _i, _p, _p, _p, _i, _i, _f, _f, _f, _p],
     "fdtd_step_fused": [ctypes.POINTER(StepArgs), _p],
     "fdtd_record_phasor64": [_p, _p, _p, _p, _p, _p, _i, _p, _i, _p, _i, _i, _i, _i, _i, _i,
                              _i, _i, _i, _i, _i, _p],

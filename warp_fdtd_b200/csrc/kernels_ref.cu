@@ -205,6 +205,38 @@ __global__ void record_curl_kernel(const float *__restrict__ h, i64 cols,
     for (int k = 0; k < 3; ++k) hist[(t * 3 + k) * dn + j] = courant * curl[k];
 }
 
+// record_curl over ping-pong, pitched buffers.
+__global__ void record_curl_pp_kernel(const float *__restrict__ H0, const float *__restrict__ H1,
+                                      int pitch, const int *__restrict__ step,
+                                      const int *__restrict__ hist_step,
+                                      float *__restrict__ hist, int nx, int ny, int nz, int x0,
+                                      int y0, int z0, int sx, int sy, int sz, float courant) {
+    const i64 dn = (i64)sx * sy * sz;
+    i64 j = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= dn) return;
+    const float *h = (step[0] & 1) ? H1 : H0;
+    const i64 cols = (i64)nx * ny * pitch;
+    int x = x0 + (int)(j / ((i64)sy * sz));
+    int y = y0 + (int)((j / sz) % sy);
+    int z = z0 + (int)(j % sz);
+    float v[3], a[3], b[3], c[3];
+    sample3(h, cols, x, y, z, nx, ny, nz, 0, v, pitch);
+    sample3(h, cols, x - 1, y, z, nx, ny, nz, 0, a, pitch);
+    sample3(h, cols, x, y - 1, z, nx, ny, nz, 0, b, pitch);
+    sample3(h, cols, x, y, z - 1, nx, ny, nz, 0, c, pitch);
+    float dx[3], dy[3], dz[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        dx[k] = v[k] - a[k];
+        dy[k] = v[k] - b[k];
+        dz[k] = v[k] - c[k];
+    }
+    float curl[3] = {dy[2] - dz[1], dz[0] - dx[2], dx[1] - dy[0]};
+    const i64 t = hist_step[0];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) hist[(t * 3 + k) * dn + j] = courant * curl[k];
+}
+
 // adjoint.py:46-88 `prepare`.
 __global__ void prepare_kernel(const float *__restrict__ q, const float *__restrict__ eps,
                                float *__restrict__ psi, const float *__restrict__ coeff,
@@ -433,6 +465,21 @@ int fdtd_record_curl(const float *h, long long cols, float *hist, const int *ste
     record_curl_kernel<<<blocks_for(dn, 256), 256, 0, as_stream(stream)>>>(
         h, cols, hist, step, nx, ny, nz, x0, y0, z0, sx, sy, sz, courant);
     return launch_status("fdtd_record_curl");
+}
+
+int fdtd_record_curl_pp(const float *H0, const float *H1, int pitch_z, const int *step,
+                        const int *hist_step, float *hist, int nx, int ny, int nz, int x0,
+                        int y0, int z0, int sx, int sy, int sz, float courant, void *stream) {
+    const i64 dn = (i64)sx * sy * sz;
+    if (pitch_z <= 0) pitch_z = nz;
+    if (dn <= 0 || !H0 || !H1 || !step || !hist_step || !hist || pitch_z < nz || x0 < 0 ||
+        y0 < 0 || z0 < 0 || x0 + sx > nx || y0 + sy > ny || z0 + sz > nz) {
+        set_error("fdtd_record_curl_pp: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    record_curl_pp_kernel<<<blocks_for(dn, 256), 256, 0, as_stream(stream)>>>(
+        H0, H1, pitch_z, step, hist_step, hist, nx, ny, nz, x0, y0, z0, sx, sy, sz, courant);
+    return launch_status("fdtd_record_curl_pp");
 }
 
 int fdtd_prepare(const float *q, const float *eps, float *psi, const float *coeff, int clen,

@@ -229,4 +229,34 @@ int fdtd_material_subpixel_adjoint(const float *rho, const float *g, float *rho_
     return launch_status("fdtd_material_subpixel_adjoint");
 }
 
+int fdtd_material_forward(const float *p, const float *weights, int radius, float *scratch,
+                          float *out, int px, int py, float beta, float eps_lo,
+                          float contrast, void *stream) {
+    if (!scratch) {
+        set_error("fdtd_material_forward: null scratch");
+        return FDTD_ERR_ARG;
+    }
+    int rc = fdtd_material_smooth(p, weights, radius, scratch, px, py, stream);
+    if (rc) return rc;
+    return fdtd_material_subpixel(scratch, out, px, py, beta, eps_lo, contrast, stream);
+}
+
+int fdtd_material_backward(const float *p, const float *weights, int radius, const float *g,
+                           float *scratch, float *p_grad, int px, int py, float beta,
+                           float eps_lo, float contrast, void *stream) {
+    if (!scratch || !p_grad || !g || px < 2 || py < 2) {
+        set_error("fdtd_material_backward: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    const size_t n = (size_t)px * py;
+    float *rho = scratch, *g_rho = scratch + n;
+    int rc = fdtd_material_smooth(p, weights, radius, rho, px, py, stream);
+    if (rc) return rc;
+    cudaMemsetAsync(g_rho, 0, n * sizeof(float), (cudaStream_t)stream);
+    cudaMemsetAsync(p_grad, 0, n * sizeof(float), (cudaStream_t)stream);
+    rc = fdtd_material_subpixel_adjoint(rho, g, g_rho, px, py, beta, eps_lo, contrast, stream);
+    if (rc) return rc;
+    return fdtd_material_smooth_adjoint(g_rho, weights, radius, p_grad, px, py, stream);
+}
+
 }  // extern "C"
