@@ -143,6 +143,26 @@ int fdtd_material_forward(const float *p, const float *weights, int radius, floa
                           float *out, int px, int py, float beta, float eps_lo,
                           float contrast, void *stream);
 
+/* fdtd_material_forward without the scratch argument, for callers that may not
+ * allocate device memory themselves: an embedding application that owns a
+ * fixed memory budget and hands the library only its input and output
+ * buffers, or a control loop where a cudaMalloc (which can synchronise the
+ * device) is not acceptable.  This entry point has no counterpart in the
+ * reference.  The smoothed density lives in a static device array built into
+ * the library, FDTD_MATERIAL_NOALLOC_MAX floats (1,048,576 = 4 MiB, held on
+ * every GPU that loads the library until the process exits); px * py above
+ * that limit is rejected with FDTD_ERR_ARG.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) with that device
+ * current, so make that first call before any stream capture.  Every call
+ * shares the one array: calls whose work overlaps on the GPU (other streams,
+ * other threads) race and must be serialised by the caller.  Nothing in the
+ * array needs clearing between calls; each call overwrites the px * py
+ * entries it uses.  Allocates nothing. */
+#define FDTD_MATERIAL_NOALLOC_MAX (1 << 20)
+int fdtd_material_forward_noalloc(const float *p, const float *weights, int radius,
+                                  float *out, int px, int py, float beta, float eps_lo,
+                                  float contrast, void *stream);
+
 /* Its pullback (material.py:93-102): p_grad = (d out / d p)^T g, overwritten.
  * scratch holds 2*px*py floats (the smoothed density and its adjoint). */
 int fdtd_material_backward(const float *p, const float *weights, int radius, const float *g,

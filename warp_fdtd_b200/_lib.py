@@ -84,6 +84,7 @@ _SIGNATURES = {
     "fdtd_material_subpixel": [_p, _p, _i, _i, _f, _f, _f, _p],
     "fdtd_material_subpixel_adjoint": [_p, _p, _p, _i, _i, _f, _f, _f, _p],
     "fdtd_material_forward": [_p, _p, _i, _p, _p, _i, _i, _f, _f, _f, _p],
+    "fdtd_material_forward_noalloc": [_p, _p, _i, _p, _i, _i, _f, _f, _f, _p],
     "fdtd_material_backward": [_p, _p, _i, _p, _p, _p, _i, _i, _f, _f, _f, _p],
     "fdtd_step_fused": [ctypes.POINTER(StepArgs), _p],
     "fdtd_record_phasor64": [_p, _p, _p, _p, _p, _p, _i, _p, _i, _p, _i, _i, _i, _i, _i, _i,

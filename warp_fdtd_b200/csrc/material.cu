@@ -2,6 +2,8 @@
 // mode.  The reference differentiates the map with a Warp Tape
 // (material.py:78-102); here the adjoint of each kernel is written out, and the
 // smoothing adjoint gathers per target pixel so its sums are deterministic.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace wfb {
@@ -174,6 +176,40 @@ __global__ void subpixel_adjoint_kernel(const float *__restrict__ rho,
     }
 }
 
+// Scratch of fdtd_material_forward_noalloc: one static array per device that
+// loads the library, shared by every call of that entry point.
+static __device__ __align__(256) float g_material_scratch[FDTD_MATERIAL_NOALLOC_MAX];
+
+// Device address of g_material_scratch on the current device, looked up once
+// per device (the host-side symbol is only a stand-in, never a device pointer).
+static int material_scratch_address(float **out) {
+    static std::mutex lock;
+    static float *cached[64] = {};
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) {
+        set_error("fdtd_material_forward_noalloc: cudaGetDevice: %s", cudaGetErrorString(err));
+        return FDTD_ERR_CUDA;
+    }
+    if (dev < 0 || dev >= 64) {
+        set_error("fdtd_material_forward_noalloc: device index %d out of range", dev);
+        return FDTD_ERR_ARG;
+    }
+    std::lock_guard<std::mutex> guard(lock);
+    if (!cached[dev]) {
+        void *ptr = nullptr;
+        err = cudaGetSymbolAddress(&ptr, g_material_scratch);
+        if (err != cudaSuccess || !ptr) {
+            set_error("fdtd_material_forward_noalloc: cudaGetSymbolAddress: %s",
+                      cudaGetErrorString(err));
+            return FDTD_ERR_CUDA;
+        }
+        cached[dev] = (float *)ptr;
+    }
+    *out = cached[dev];
+    return FDTD_OK;
+}
+
 }  // namespace wfb
 
 using namespace wfb;
@@ -239,6 +275,32 @@ int fdtd_material_forward(const float *p, const float *weights, int radius, floa
     int rc = fdtd_material_smooth(p, weights, radius, scratch, px, py, stream);
     if (rc) return rc;
     return fdtd_material_subpixel(scratch, out, px, py, beta, eps_lo, contrast, stream);
+}
+
+int fdtd_material_forward_noalloc(const float *p, const float *weights, int radius,
+                                  float *out, int px, int py, float beta, float eps_lo,
+                                  float contrast, void *stream) {
+    if (!p || !weights || !out || px < 2 || py < 2 || radius < 0 || !(beta > 0.0f)) {
+        set_error("fdtd_material_forward_noalloc: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    if ((long long)px * py > FDTD_MATERIAL_NOALLOC_MAX) {
+        set_error("fdtd_material_forward_noalloc: %d x %d pixels exceed the built-in scratch "
+                  "of %d floats; use fdtd_material_forward with caller scratch",
+                  px, py, FDTD_MATERIAL_NOALLOC_MAX);
+        return FDTD_ERR_ARG;
+    }
+    float *scratch = nullptr;
+    int rc = material_scratch_address(&scratch);
+    if (rc) return rc;
+    const int n = px * py;
+    smooth_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(p, weights, radius,
+                                                                     scratch, px, py);
+    rc = launch_status("fdtd_material_forward_noalloc (smooth)");
+    if (rc) return rc;
+    subpixel_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(scratch, out, px, py,
+                                                                       beta, eps_lo, contrast);
+    return launch_status("fdtd_material_forward_noalloc (subpixel)");
 }
 
 int fdtd_material_backward(const float *p, const float *weights, int radius, const float *g,
