@@ -31,7 +31,7 @@ struct FzLayout {
     int off_h, off_e, off_m, off_pze, off_pzh;  // byte offsets inside a stage
     int stage_bytes;
     unsigned tx_bytes;
-    int off_stages, off_ring, RW, off_coef, off_mtab, smem_bytes;
+    int off_stages, off_ring, RW, off_coef, XK, off_mtab, smem_bytes;
 };
 
 struct FzMaps {
@@ -126,6 +126,64 @@ __device__ __forceinline__ void cpml_axis(VF<V> &d0, VF<V> &d1, float4 c, const 
     }
 }
 
+// The same with the old psi values already in registers (p0 / p1 are read
+// only where c.x != 0, which is where they were loaded).
+template <int V>
+__device__ __forceinline__ void cpml_axis_r(VF<V> &d0, VF<V> &d1, float4 c, const VF<V> &p0,
+                                            const VF<V> &p1, float *pn, i64 ib, i64 slot,
+                                            bool own) {
+    VF<V> n0 = zero_v<V>(), n1 = zero_v<V>();
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+        d0.v[j] = cpml1(d0.v[j], c, p0.v[j], n0.v[j]);
+        d1.v[j] = cpml1(d1.v[j], c, p1.v[j], n1.v[j]);
+    }
+    if (own && c.x != 0.0f) {
+        stv<V>(pn + ib, n0);
+        stv<V>(pn + ib + slot, n1);
+    }
+}
+
+// CPML filter of a cell group along z: per-cell coefficients from `cz`, the
+// group's old psi pair staged at `po0` / `po1` (slab ranks rb .. rb+V-1), new
+// values to `pn + ib` and `pn + ib + slot` if `store`.  Inactive cells of a
+// slab window keep psi at zero.
+template <int V>
+__device__ __forceinline__ void cpml_z(VF<V> &d0, VF<V> &d1, const float4 *cz, bool has_psi,
+                                       const float *po0, const float *po1, float *pn, i64 ib,
+                                       i64 slot, bool store) {
+    VF<V> z0, z1, u0 = zero_v<V>(), u1 = zero_v<V>();
+    if (has_psi) {
+        z0 = ldsv<V>(po0);
+        z1 = ldsv<V>(po1);
+    }
+#pragma unroll
+    for (int j = 0; j < V; ++j) {
+        const float4 c = cz[j];
+        d0.v[j] = cpml1(d0.v[j], c, z0.v[j], u0.v[j]);
+        d1.v[j] = cpml1(d1.v[j], c, z1.v[j], u1.v[j]);
+    }
+    if (store && has_psi) {
+        stv<V>(pn + ib, u0);
+        stv<V>(pn + ib + slot, u1);
+    }
+}
+
+// A cell group with z-slab psi must hold the aligned consecutive slab ranks
+// rb .. rb+V-1 (one vector of the staged z-slab rows) inside the slab width.
+template <int V>
+__device__ __forceinline__ bool group_ranks_ok(const float4 *tab, int RZ) {
+    const int rb = (int)tab[0].w;
+    bool psi = false, ok = true;
+#pragma unroll
+    for (int j = 0; j < V; ++j)
+        if (tab[j].x != 0.0f) {
+            psi = true;
+            ok &= (int)tab[j].w == rb + j;
+        }
+    return !psi || (ok && rb % V == 0 && rb + V <= RZ);
+}
+
 template <int MAT, int S, int V>
 __global__ void __launch_bounds__(512)
     fz_step_kernel(const __grid_constant__ FzMaps maps, const __grid_constant__ FzParams prm) {
@@ -139,14 +197,18 @@ __global__ void __launch_bounds__(512)
     const int HS = (TY + 2) * HB;   // H component stride in a stage
     const int ES = (TY + 1) * P;    // E component stride in a stage
     const int RS = (TY + 1) * RW;   // ring component stride
+    const int lanes = P / V;
 
     uint64_t *bars = (uint64_t *)smem;
+    int *meta = (int *)(smem + 64);  // [0] slab rank check failed
     unsigned char *stage0 = smem + L.off_stages;
     float *ring = (float *)(smem + L.off_ring);  // [2][3][TY+1][RW]
     float4 *cey = (float4 *)(smem + L.off_coef);
     float4 *chy = cey + (TY + 1);
     float4 *cez = chy + (TY + 1);
     float4 *chz = cez + P;
+    float4 *cex = chz + P;   // by stage index k: E coefficient of plane xa-1+k
+    float4 *chx = cex + L.XK;  // ... H coefficient of plane xa-2+k
     float *mtab = (float *)(smem + L.off_mtab);
 
     const int tiles_y = (ny + TY - 1) / TY;
@@ -170,10 +232,7 @@ __global__ void __launch_bounds__(512)
     const float4 *__restrict__ ch = (const float4 *)a.coeff_h;
     const int clen = a.clen;
     const float courant = a.courant;
-    const int lx = threadIdx.x, ly = threadIdx.y;
-    const int tid = ly * blockDim.x + lx, nth = blockDim.x * blockDim.y;
-    const int zv = lx * V;        // first of this thread's V z cells
-    const int gy = y0 + ly;       // this thread's row (E: ly <= TY, H: ly < TY)
+    const int tid = threadIdx.x, nth = blockDim.x;
     const bool wave_ok = t >= 0 && t < a.waves_cols;
     const i64 xslot = (i64)a.psi_rx * plane;      // slot stride of the X block
     const i64 yslot = (i64)a.psi_ry * nx * P;     // ... of the Y block
@@ -190,7 +249,7 @@ __global__ void __launch_bounds__(512)
         tma_load_3d(st + L.off_m, &maps.M, 0, y0, p, bar);
         if (RZ > 0) {
             tma_load_4d(st + L.off_pze, &maps.PZE[s], 0, y0, p, 0, bar);
-            tma_load_4d(st + L.off_pzh, &maps.PZH[s], 0, y0, p, 0, bar);
+            tma_load_4d(st + L.off_pzh, &maps.PZH[s], 0, y0, p - 1, 0, bar);
         }
     };
 
@@ -211,21 +270,43 @@ __global__ void __launch_bounds__(512)
         cez[j] = j < nz ? __ldg(ce + 2 * clen + j) : ident;
         chz[j] = j < nz ? __ldg(ch + 2 * clen + j) : ident;
     }
+    for (int j = tid; j <= last; j += nth) {
+        const int p = xa - 1 + j;
+        cex[j] = p >= 0 && p < nx ? __ldg(ce + p) : ident;
+        chx[j] = p >= 1 && p - 1 < nx ? __ldg(ch + p - 1) : ident;
+    }
     // the ring's +z pad columns (z = P .. P+3) are the zero padding beyond the grid
     for (int j = tid; j < 2 * 3 * (TY + 1) * 4; j += nth) {
         const int r = j >> 2, c = j & 3;
         ring[r * RW + P + c] = 0.0f;
     }
     __syncthreads();
+    if (tid == 0) {
+        int bad = 0;
+        for (int l = 0; l < lanes; ++l)
+            if (!(group_ranks_ok<V>(cez + l * V, RZ) && group_ranks_ok<V>(chz + l * V, RZ))) bad = 1;
+        meta[0] = bad;
+    }
+    __syncthreads();
+    if (meta[0]) {
+        if (tid == 0 && a.error) atomicExch(a.error, 2);
+        return;  // nothing issued yet
+    }
+    const int ly = tid / lanes;           // this thread's row (E: ly <= TY, H: ly < TY)
+    const int zv = (tid - ly * lanes) * V;  // first of this thread's V z cells
+    const int gy = y0 + ly;
     // per-thread CPML activity of its row and its z cells
     const float4 my_cey = cey[ly], my_chy = chy[min(ly, TY - 1)];
     const bool yE = active(my_cey), yH = ly < TY && active(my_chy);
-    bool zE = false, zH = false;
+    bool zE = false, zH = false, zEp = false, zHp = false;
 #pragma unroll
     for (int j = 0; j < V; ++j) {
         zE |= active(cez[zv + j]);
         zH |= active(chz[zv + j]);
+        zEp |= cez[zv + j].x != 0.0f;
+        zHp |= chz[zv + j].x != 0.0f;
     }
+    const int rbe = (int)cez[zv].w, rbh = (int)chz[zv].w;
 
     int issued;
     if (tid == 0)
@@ -244,10 +325,37 @@ __global__ void __launch_bounds__(512)
     const int r_off = ly * RW + zv;            // ... in the E ring
     const int g_off = gy * P + zv;             // ... in a field plane (elements)
     const bool row_in = gy < ny;
+    // H of the previous plane at this thread's cells: the E update's x
+    // difference and the H update's old value, so a stage is free as soon as
+    // the plane after it starts
+    VF<V> hprev[3];
+    {
+        const float *H0 = (const float *)(stage0 + L.off_h);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) hprev[c] = ldsv<V>(H0 + c * HS + h_off);
+    }
+    const int issuer = nth - 1;  // a thread of row TY, which has no H update
 
     int k = 1;
     for (; k <= last; ++k) {
         const int p = xa - 1 + k;
+        const int q = p - 1;
+        const float4 cxh = chx[k];
+        const bool h_on = q >= xa && ly < TY && row_in;
+        // x- and y-slab psi of the H plane q: in flight during the E update
+        VF<V> xh0, xh1, yh0, yh1;
+        if (h_on) {
+            if (cxh.x != 0.0f) {
+                const i64 ib = prm.xoff + ((i64)(int)cxh.w * ny + gy) * P + zv;
+                xh0 = ldgv<V>(ph_o + ib);
+                xh1 = ldgv<V>(ph_o + ib + xslot);
+            }
+            if (my_chy.x != 0.0f) {
+                const i64 ib = prm.yoff + ((i64)(int)my_chy.w * nx + q) * P + zv;
+                yh0 = ldgv<V>(ph_o + ib);
+                yh1 = ldgv<V>(ph_o + ib + yslot);
+            }
+        }
         if (!timed_out) {
             if (mbar_wait_bounded(bars + (k % S), (k / S) & 1, limit))
                 done = k;
@@ -255,27 +363,25 @@ __global__ void __launch_bounds__(512)
                 timed_out = true;
         }
         const unsigned char *stc = stage_ptr(k);
-        const unsigned char *stp = stage_ptr(k - 1);
         float *Rc = ring + (k & 1) * 3 * RS;
         // ---------------- E update, rows y0 .. y0+TY ----------------
         if (!timed_out) {
             VF<V> o[3] = {zero_v<V>(), zero_v<V>(), zero_v<V>()};
             if (p < nx && row_in) {
                 const float *Hc = (const float *)(stc + L.off_h);
-                const float *Hp = (const float *)(stp + L.off_h);
                 const float *Eo = (const float *)(stc + L.off_e);
                 VF<V> dx[3], dy[3], dz[3];
 #pragma unroll
-                for (int q = 0; q < 3; ++q) {
-                    const VF<V> hc = ldsv<V>(Hc + q * HS + h_off);
-                    const VF<V> hp = ldsv<V>(Hp + q * HS + h_off);
-                    const VF<V> hy = ldsv<V>(Hc + q * HS + h_off - HB);
-                    float zm = Hc[q * HS + h_off - 1];
+                for (int q3 = 0; q3 < 3; ++q3) {
+                    const VF<V> hc = ldsv<V>(Hc + q3 * HS + h_off);
+                    const VF<V> &hp = hprev[q3];
+                    const VF<V> hy = ldsv<V>(Hc + q3 * HS + h_off - HB);
+                    float zm = Hc[q3 * HS + h_off - 1];
 #pragma unroll
                     for (int j = 0; j < V; ++j) {
-                        dx[q].v[j] = hc.v[j] - hp.v[j];
-                        dy[q].v[j] = hc.v[j] - hy.v[j];
-                        dz[q].v[j] = hc.v[j] - zm;
+                        dx[q3].v[j] = hc.v[j] - hp.v[j];
+                        dy[q3].v[j] = hc.v[j] - hy.v[j];
+                        dz[q3].v[j] = hc.v[j] - zm;
                         zm = hc.v[j];
                     }
                 }
@@ -294,10 +400,10 @@ __global__ void __launch_bounds__(512)
 #pragma unroll
                     for (int j = 0; j < V; ++j) ie[j] = t4.v[j];
                 }
-                const float4 cx = __ldg(ce + p);
+                const float4 cx = cex[k];
                 const bool own = p < xb && ly < TY;
                 // CPML filter per axis (kernels.py:113-118): x is uniform over the
-                // block's plane, y over the thread's row, z only in slab lanes.
+                // block's plane, y over the thread's row, z per cell of the group.
                 // dx[2] = dxz, dx[1] = dxy, dy[0] = dyx, dy[2] = dyz, dz[1] = dzy, dz[0] = dzx
                 if (active(cx))
                     cpml_axis<V>(dx[2], dx[1], cx, pe_o, pe_n,
@@ -307,23 +413,9 @@ __global__ void __launch_bounds__(512)
                                  prm.yoff + ((i64)(int)my_cey.w * nx + p) * P + zv, yslot, own);
                 if (zE) {
                     const float *pz = (const float *)(stc + L.off_pze);  // [2][TY+1][RZ]
-#pragma unroll
-                    for (int j = 0; j < V; ++j) {
-                        const float4 cz = cez[zv + j];
-                        float z4 = 0.0f, z5 = 0.0f, u4 = 0.f, u5 = 0.f;
-                        const int rz = (int)cz.w;
-                        if (cz.x != 0.0f) {
-                            z4 = pz[ly * RZ + rz];
-                            z5 = pz[(TY + 1) * RZ + ly * RZ + rz];
-                        }
-                        dz[1].v[j] = cpml1(dz[1].v[j], cz, z4, u4);
-                        dz[0].v[j] = cpml1(dz[0].v[j], cz, z5, u5);
-                        if (own && cz.x != 0.0f && zv + j < nz) {
-                            const i64 zb = prm.zoff + ((i64)p * ny + gy) * RZ + rz;
-                            pe_n[zb] = u4;
-                            pe_n[zb + zslot] = u5;
-                        }
-                    }
+                    cpml_z<V>(dz[1], dz[0], cez + zv, zEp, pz + ly * RZ + rbe,
+                              pz + (TY + 1) * RZ + ly * RZ + rbe, pe_n,
+                              prm.zoff + ((i64)p * ny + gy) * RZ + rbe, zslot, own);
                 }
                 const VF<V> e0 = ldsv<V>(Eo + e_off), e1 = ldsv<V>(Eo + ES + e_off),
                             e2 = ldsv<V>(Eo + 2 * ES + e_off);
@@ -360,9 +452,13 @@ __global__ void __launch_bounds__(512)
             timed_out = true;
             break;
         }
+        // plane k-1's stage is no longer read: refill it while the H update runs
+        if (k - 1 + S <= last) {
+            if (tid == issuer) issue(k - 1 + S);
+            issued = k - 1 + S;
+        }
         // ---------------- H update at plane q = p - 1, rows y0 .. y0+TY-1 ----------------
-        const int q = p - 1;
-        if (q >= xa && ly < TY && row_in) {
+        if (h_on) {
             const float *Rq = ring + ((k - 1) & 1) * 3 * RS;
             VF<V> dx[3], dy[3], dz[3];
 #pragma unroll
@@ -379,36 +475,19 @@ __global__ void __launch_bounds__(512)
                     dz[r].v[j] = nxt - eq.v[j];
                 }
             }
-            const float4 cx = __ldg(ch + q);
-            if (active(cx))
-                cpml_axis<V>(dx[2], dx[1], cx, ph_o, ph_n,
-                             prm.xoff + ((i64)(int)cx.w * ny + gy) * P + zv, xslot, true);
+            if (active(cxh))
+                cpml_axis_r<V>(dx[2], dx[1], cxh, xh0, xh1, ph_n,
+                               prm.xoff + ((i64)(int)cxh.w * ny + gy) * P + zv, xslot, true);
             if (yH)
-                cpml_axis<V>(dy[0], dy[2], my_chy, ph_o, ph_n,
-                             prm.yoff + ((i64)(int)my_chy.w * nx + q) * P + zv, yslot, true);
+                cpml_axis_r<V>(dy[0], dy[2], my_chy, yh0, yh1, ph_n,
+                               prm.yoff + ((i64)(int)my_chy.w * nx + q) * P + zv, yslot, true);
             if (zH) {
-                const float *pz = (const float *)(stp + L.off_pzh);  // [2][TY][RZ]
-#pragma unroll
-                for (int j = 0; j < V; ++j) {
-                    const float4 cz = chz[zv + j];
-                    float z4 = 0.0f, z5 = 0.0f, u4 = 0.f, u5 = 0.f;
-                    const int rz = (int)cz.w;
-                    if (cz.x != 0.0f) {
-                        z4 = pz[ly * RZ + rz];
-                        z5 = pz[TY * RZ + ly * RZ + rz];
-                    }
-                    dz[1].v[j] = cpml1(dz[1].v[j], cz, z4, u4);
-                    dz[0].v[j] = cpml1(dz[0].v[j], cz, z5, u5);
-                    if (cz.x != 0.0f && zv + j < nz) {
-                        const i64 zb = prm.zoff + ((i64)q * ny + gy) * RZ + rz;
-                        ph_n[zb] = u4;
-                        ph_n[zb + zslot] = u5;
-                    }
-                }
+                const float *pz = (const float *)(stc + L.off_pzh);  // [2][TY][RZ], plane q
+                cpml_z<V>(dz[1], dz[0], chz + zv, zHp, pz + ly * RZ + rbh,
+                          pz + TY * RZ + ly * RZ + rbh, ph_n,
+                          prm.zoff + ((i64)q * ny + gy) * RZ + rbh, zslot, true);
             }
-            const float *Hq = (const float *)(stp + L.off_h);
-            const VF<V> h0 = ldsv<V>(Hq + h_off), h1 = ldsv<V>(Hq + HS + h_off),
-                        h2 = ldsv<V>(Hq + 2 * HS + h_off);
+            const VF<V> &h0 = hprev[0], &h1 = hprev[1], &h2 = hprev[2];
             VF<V> o[3];
 #pragma unroll
             for (int j = 0; j < V; ++j) {
@@ -431,11 +510,12 @@ __global__ void __launch_bounds__(512)
             stv<V>(dst + cols, o[1]);
             stv<V>(dst + 2 * cols, o[2]);
         }
-        __syncthreads();
-        if (k - 1 + S <= last) {
-            if (tid == 0) issue(k - 1 + S);
-            issued = k - 1 + S;
+        {
+            const float *Hc = (const float *)(stc + L.off_h);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) hprev[c] = ldsv<V>(Hc + c * HS + h_off);
         }
+        __syncthreads();
     }
     if (timed_out) {
         if (tid == 0) {
@@ -449,7 +529,7 @@ __global__ void __launch_bounds__(512)
 
 static inline size_t up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-static FzLayout fz_layout(int ty, int P, int RZ, int S, int mat) {
+static FzLayout fz_layout(int ty, int P, int RZ, int S, int mat, int chunk_x) {
     FzLayout L;
     L.ty = ty;
     L.P = P;
@@ -474,7 +554,8 @@ static FzLayout fz_layout(int ty, int P, int RZ, int S, int mat) {
     L.off_ring = (int)(L.off_stages + (size_t)S * L.stage_bytes);
     size_t ring = (size_t)2 * 3 * (ty + 1) * L.RW * 4;
     L.off_coef = (int)up(L.off_ring + ring, 16);
-    size_t coef = (size_t)(2 * (ty + 1) + 2 * P) * 16;
+    L.XK = chunk_x + 2;  // x coefficients of planes xa-1 .. xb (E) and xa-2 .. xb-1 (H)
+    size_t coef = (size_t)(2 * (ty + 1) + 2 * P + 2 * L.XK) * 16;
     L.off_mtab = (int)up(L.off_coef + coef, 16);
     L.smem_bytes = (int)(L.off_mtab + (mat == 1 ? 256 * 4 : 0));
     return L;
@@ -500,8 +581,8 @@ int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
         set_error("fdtd_step_fused: full-z path takes 2..4 stages");
         return FDTD_ERR_ARG;
     }
-    FzLayout L = fz_layout(ty, P, RZ, S, a.material_kind);
-    while (L.smem_bytes > 220 * 1024 && S > 2) L = fz_layout(ty, P, RZ, --S, a.material_kind);
+    FzLayout L = fz_layout(ty, P, RZ, S, a.material_kind, a.chunk_x);
+    while (L.smem_bytes > 220 * 1024 && S > 2) L = fz_layout(ty, P, RZ, --S, a.material_kind, a.chunk_x);
     const int V = a.vector == 2 ? 2 : 4;
     const int lanes = P / V;
     if (L.smem_bytes > 220 * 1024 || lanes * (ty + 1) > 512 || ty + 2 > 256) {
@@ -561,7 +642,7 @@ int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
     const int tiles = (a.ny + ty - 1) / ty;
     const int chunks = (a.nx + a.chunk_x - 1) / a.chunk_x;
     dim3 grid((unsigned)(tiles * chunks));
-    dim3 threads((unsigned)lanes, (unsigned)(ty + 1));
+    dim3 threads((unsigned)(lanes * (ty + 1)));
 #define LAUNCH3(M, SS, W)                                                                    \
     do {                                                                                     \
         cudaFuncSetAttribute(fz_step_kernel<M, SS, W>,                                       \

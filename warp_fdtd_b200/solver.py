@@ -45,6 +45,40 @@ def pack_coefficients(coeff, shape):
     return packed, max(1, *slab_sizes)
 
 
+def slab_ranks(packed, shape):
+    """Ranks of the slab psi layout (the full-z pipeline's own layout).
+
+    Per axis, each CPML side is one window running from its first to its last
+    active cell (the low side holds the active cells in the lower half of the
+    axis, the high side the rest); z windows are widened to whole groups of
+    four cells so a group's four psi values are one aligned 16-byte vector.
+    Every cell of a window, active or not, is numbered consecutively, windows
+    one after the other, so a tile of rows inside a window has affine ranks.
+    Returns the table with column 3 replaced and the three window lengths."""
+    out = packed.copy()
+    out[..., 3] = 0
+    lengths = []
+    for axis, length in enumerate(shape):
+        act = np.flatnonzero(packed[axis, :length, 0] != 0)
+        half = (length + 1) // 2
+        wins = []
+        for side in (act[act < half], act[act >= half]):
+            if len(side):
+                lo, hi = int(side[0]), int(side[-1])
+                if axis == 2:
+                    lo, hi = lo // 4 * 4, hi // 4 * 4 + 3
+                wins.append([lo, hi])
+        if len(wins) == 2 and wins[1][0] <= wins[0][1] + 1:
+            wins = [[wins[0][0], wins[1][1]]]
+        rank = 0
+        for lo, hi in wins:
+            idx = np.arange(lo, min(hi + 1, out.shape[1]))
+            out[axis, idx, 3] = rank + idx - lo
+            rank += hi - lo + 1
+        lengths.append(rank)
+    return out, lengths
+
+
 def owned_array_bytes(solver):
     """solver.py:32-50: live owned device-tensor storage (deduplicated by pointer).
 
@@ -206,8 +240,13 @@ class Solver:
         active = [max(int((packed[f][0][axis, :self.shape[axis], 0] != 0).sum()) for f in "EH")
                   for axis in range(3)]
         self._psi_r = (active[0], active[1], (active[2] + 3) // 4 * 4)
+        # the table the fused step reads: reference plane ranks, or slab ranks
+        self._coeff_step = self._coeff4
         if use_slab:
             self._psi_layout = 2
+            slab = {f: slab_ranks(packed[f][0], self.shape) for f in "EH"}
+            self._coeff_step = {f: torch.from_numpy(slab[f][0]).to(dev) for f in "EH"}
+            self._psi_r = tuple(max(slab["E"][1][a], slab["H"][1][a]) for a in range(3))
             rx, ry, rz = self._psi_r
             self._psi_cols = max(1, 2 * rx * ny * self._pitch + 2 * ry * nx * self._pitch
                                  + 2 * nx * ny * rz)
@@ -303,7 +342,7 @@ class Solver:
         nx, ny, nz = self.shape
         P = self._pitch
         rx, ry, rz = self._psi_r
-        c4 = self._coeff4[field].cpu()
+        c4 = self._coeff_step[field].cpu()
         full = torch.zeros((6, nx, ny, nz), dtype=torch.float32, device=self.device)
         xb = buf[: 2 * rx * ny * P].view(2, rx, ny, P)
         yb = buf[2 * rx * ny * P: 2 * rx * ny * P + 2 * ry * nx * P].view(2, ry, nx, P)
@@ -349,8 +388,8 @@ class Solver:
             a.psi_h[j] = ptr(self._psi_h[j])
         a.psi_cols = self._psi_cols
         a.psi_rx, a.psi_ry, a.psi_rz = self._psi_r
-        a.coeff_e = ptr(self._coeff4["E"])
-        a.coeff_h = ptr(self._coeff4["H"])
+        a.coeff_e = ptr(self._coeff_step["E"])
+        a.coeff_h = ptr(self._coeff_step["H"])
         a.clen = int(self._coeff4["E"].shape[1])
         a.packed = int(self._psi_layout)
         a.material_kind = self.material_kind
