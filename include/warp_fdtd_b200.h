@@ -195,7 +195,12 @@ int fdtd_material_backward(const float *p, const float *weights, int radius, con
  *                  (psi_rz a multiple of 4); the slot pair of each axis is
  *                  (2*axis, 2*axis+1) and ranks come from coeff[...][3].  The
  *                  Z block is contiguous in z-rank so the full-z TMA path can
- *                  stage it with the fields. */
+ *                  stage it with the fields.  Slab ranks are this layout's
+ *                  own: every cell of a z window of active cells, widened to
+ *                  whole groups of 4 (V) cells, gets consecutive ranks, so the
+ *                  4 cells of a group with any active cell hold ranks
+ *                  rb .. rb+3 with rb % 4 == 0 and rb + 4 <= psi_rz; a block
+ *                  that finds otherwise sets *error = 2 and writes nothing. */
 #define FDTD_PSI_FULL 0
 #define FDTD_PSI_PACKED 1
 #define FDTD_PSI_SLAB 2
@@ -233,9 +238,19 @@ typedef struct fdtd_step_args {
     int vector;                /* TMA path: z cells per thread (1, 2, 4); 0 picks */
     int stages;                /* TMA path: planes in the load ring (2..8); 0 picks */
     int *error;                /* optional device int, set to 1 if a bounded wait expires */
+    const int *schedule;       /* path 3, optional: schedule_blocks int4 entries in device
+                                  memory, one per block: (y tile index, first x plane,
+                                  end x plane, 0); null keeps the tile x chunk_x grid.
+                                  chunk_x must be >= the longest entry's planes */
+    int schedule_blocks;
 } fdtd_step_args;
 
 int fdtd_step_fused(const fdtd_step_args *args, void *stream);
+
+/* Resident blocks per SM of the full-z path's kernel for these arguments
+ * (after the defaults fdtd_step_fused would pick) and the device's SM count,
+ * for sizing a schedule to whole waves.  No reference counterpart. */
+int fdtd_step_occupancy(const fdtd_step_args *args, int *blocks_per_sm, int *sms);
 
 /* Float64 running DFT at one detector plane for K frequencies (the phasor
  * branch of detectors.py:65-106 generalised), run after fdtd_step_fused and

@@ -29,6 +29,9 @@ CASES = [
     ((24, 12, 148), 8, 7, ((3, 3), (2, 2), (6, 6)), 3, "u8", False),
     ((13, 11, 36), 14, 1, ((2, 3), (3, 2), (2, 2)), 30, "u8", True),
     ((24, 12, 148), 8, 7, ((3, 3), (2, 2), (6, 6)), 30, "f32", False),
+    # path 31: path 3 over the uniform chunk grid instead of the balanced schedule
+    ((13, 11, 36), 14, 1, ((2, 3), (3, 2), (2, 2)), 31, "u8", False),
+    ((24, 12, 148), 8, 7, ((3, 3), (2, 2), (6, 6)), 31, "f32", True),
 ]
 
 
@@ -41,7 +44,8 @@ def test_solver_path_matches_oracle(tmp_path, shape, steps, seed, slabs, path, m
     case = make_bundle(tmp_path / "b", shape, steps, seed=seed, slabs=slabs, kappa=kappa)
     o = OracleSolver(case).attach()
     o.run()
-    s = Solver(case, path=3 if path == 30 else path, material=material)
+    s = Solver(case, path=3 if path in (30, 31) else path, material=material,
+               schedule="uniform" if path == 31 else "balanced")
     if path == 30:
         s._args.vector = 2
     attach(s)

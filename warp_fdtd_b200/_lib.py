@@ -63,6 +63,8 @@ class StepArgs(ctypes.Structure):
         ("vector", _i),
         ("stages", _i),
         ("error", _p),
+        ("schedule", _p),
+        ("schedule_blocks", _i),
     ]
 
 
@@ -71,6 +73,7 @@ _SIGNATURES = {
     "fdtd_update": [_i, _i, _p, _p, _ll, _p, _p, _ll, _p, _i, _p, _ll, _p, _ll, _p, _p, _ll,
                     _i, _i, _i, _i, _i, _f, _i, _p],
     "fdtd_advance": [_p, _i, _p],
+    "fdtd_step_occupancy": [ctypes.POINTER(StepArgs), _p, _p],
     "fdtd_record": [_p, _p, _p, _ll, _p, _p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i,
                     _i, _i, _i, _i, _p],
     "fdtd_record_curl": [_p, _ll, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i, _f, _p],

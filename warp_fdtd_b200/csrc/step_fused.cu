@@ -362,15 +362,12 @@ extern "C" int fdtd_step_fused(const fdtd_step_args *args, void *stream) {
     }
     cudaStream_t st = (cudaStream_t)stream;
     if (path == 3) {
-        if (a.tile_y <= 0) a.tile_y = 5;
-        const int tiles = (a.ny + a.tile_y - 1) / a.tile_y;
-        if (a.chunk_x <= 0) {
-            // about three waves of two resident blocks per SM, chunks of >= 16 planes
-            int want = 148 * 2 * 3;
-            int chunks = (want + tiles - 1) / tiles;
-            a.chunk_x = (a.nx + chunks - 1) / chunks;
-            if (a.chunk_x < 16) a.chunk_x = 16 < a.nx ? 16 : a.nx;
+        if (a.schedule && (a.schedule_blocks < 1 || a.chunk_x < 1)) {
+            set_error("fdtd_step_fused: a schedule needs schedule_blocks >= 1 and chunk_x >= "
+                      "its longest entry");
+            return FDTD_ERR_ARG;
         }
+        fz_defaults(a);
         if (a.tile_y < 1 || a.chunk_x < 1) {
             set_error("fdtd_step_fused: invalid tile");
             return FDTD_ERR_ARG;
@@ -440,4 +437,27 @@ extern "C" int fdtd_step_fused(const fdtd_step_args *args, void *stream) {
     }
 #undef LAUNCH
     return launch_status("fdtd_step_fused");
+}
+
+extern "C" int fdtd_step_occupancy(const fdtd_step_args *args, int *blocks_per_sm, int *sms) {
+    if (!args || !blocks_per_sm || !sms) {
+        set_error("fdtd_step_occupancy: null argument");
+        return FDTD_ERR_ARG;
+    }
+    fdtd_step_args a = *args;
+    if (a.pitch_z <= 0) a.pitch_z = a.nz;
+    if (a.material_pitch <= 0) a.material_pitch = a.nz;
+    if (a.nx <= 0 || a.ny <= 0 || a.nz <= 0 || a.packed != FDTD_PSI_SLAB || !fz_eligible(a)) {
+        set_error("fdtd_step_occupancy: arguments do not select the full-z path");
+        return FDTD_ERR_ARG;
+    }
+    fz_defaults(a);
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err == cudaSuccess) err = cudaDeviceGetAttribute(sms, cudaDevAttrMultiProcessorCount, dev);
+    if (err != cudaSuccess) {
+        set_error("fdtd_step_occupancy: %s", cudaGetErrorString(err));
+        return FDTD_ERR_CUDA;
+    }
+    return fz_occupancy(a, blocks_per_sm);
 }

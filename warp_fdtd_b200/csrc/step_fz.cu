@@ -212,12 +212,25 @@ __global__ void __launch_bounds__(512)
     float *mtab = (float *)(smem + L.off_mtab);
 
     const int tiles_y = (ny + TY - 1) / TY;
-    const int tyi = blockIdx.x % tiles_y;
-    const int chunk = blockIdx.x / tiles_y;
+    int tyi, xa, xb;
+    if (a.schedule) {
+        // one (y tile, x range) entry per block; reject entries outside the grid
+        // or longer than the chunk the shared-memory layout was sized for
+        const int4 seg = ((const int4 *)a.schedule)[blockIdx.x];
+        tyi = seg.x;
+        xa = seg.y;
+        xb = seg.z;
+        if (tyi < 0 || tyi >= tiles_y || xa < 0 || xb > nx || xb - xa > a.chunk_x) {
+            if (threadIdx.x == 0 && a.error) atomicExch(a.error, 3);
+            return;
+        }
+    } else {
+        tyi = blockIdx.x % tiles_y;
+        xa = (blockIdx.x / tiles_y) * a.chunk_x;
+        xb = min(xa + a.chunk_x, nx);
+    }
+    if (xa >= xb) return;
     const int y0 = tyi * TY;
-    const int xa = chunk * a.chunk_x;
-    if (xa >= nx) return;
-    const int xb = min(xa + a.chunk_x, nx);
     const int last = xb - xa + 1;  // planes k = 0..last are xa-1 .. xb
 
     const int t = a.step[0];
@@ -572,24 +585,73 @@ bool fz_eligible(const fdtd_step_args &a) {
     return a.material_kind == 1 ? al16(a.material) : al16(a.inv_eps);
 }
 
-int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
-    int rc = get_encoder();
-    if (rc) return rc;
+void fz_defaults(fdtd_step_args &a) {
+    if (a.tile_y <= 0) a.tile_y = 5;
+    if (a.chunk_x <= 0 && !a.schedule) {
+        // about three waves of two resident blocks per SM, chunks of >= 16 planes
+        const int tiles = (a.ny + a.tile_y - 1) / a.tile_y;
+        const int want = 148 * 2 * 3;
+        const int chunks = (want + tiles - 1) / tiles;
+        a.chunk_x = (a.nx + chunks - 1) / chunks;
+        if (a.chunk_x < 16) a.chunk_x = 16 < a.nx ? 16 : a.nx;
+    }
+}
+
+using FzKernel = void (*)(FzMaps, FzParams);
+
+template <int M, int SS>
+static FzKernel fz_pick_v(int V) {
+    return V == 4 ? fz_step_kernel<M, SS, 4> : fz_step_kernel<M, SS, 2>;
+}
+
+static FzKernel fz_pick(int mat, int S, int V) {
+    if (mat == 1) return S == 2 ? fz_pick_v<1, 2>(V) : S == 3 ? fz_pick_v<1, 3>(V) : fz_pick_v<1, 4>(V);
+    return S == 2 ? fz_pick_v<0, 2>(V) : S == 3 ? fz_pick_v<0, 3>(V) : fz_pick_v<0, 4>(V);
+}
+
+// Layout, stage count, z cells per thread and threads per block of a launch.
+static int fz_shape(const fdtd_step_args &a, FzLayout &L, int &S, int &V, int &threads) {
     const int P = a.pitch_z, ty = a.tile_y, RZ = a.psi_rz;
-    int S = a.stages > 0 ? a.stages : 3;
+    S = a.stages > 0 ? a.stages : 3;
     if (S < 2 || S > 4) {
         set_error("fdtd_step_fused: full-z path takes 2..4 stages");
         return FDTD_ERR_ARG;
     }
-    FzLayout L = fz_layout(ty, P, RZ, S, a.material_kind, a.chunk_x);
+    L = fz_layout(ty, P, RZ, S, a.material_kind, a.chunk_x);
     while (L.smem_bytes > 220 * 1024 && S > 2) L = fz_layout(ty, P, RZ, --S, a.material_kind, a.chunk_x);
-    const int V = a.vector == 2 ? 2 : 4;
-    const int lanes = P / V;
-    if (L.smem_bytes > 220 * 1024 || lanes * (ty + 1) > 512 || ty + 2 > 256) {
+    V = a.vector == 2 ? 2 : 4;
+    threads = P / V * (ty + 1);
+    if (L.smem_bytes > 220 * 1024 || threads > 512 || ty + 2 > 256) {
         set_error("fdtd_step_fused: full-z tile of %d rows does not fit (%d bytes, %d threads)", ty,
-                  L.smem_bytes, lanes * (ty + 1));
+                  L.smem_bytes, threads);
         return FDTD_ERR_ARG;
     }
+    return 0;
+}
+
+int fz_occupancy(const fdtd_step_args &a, int *blocks_per_sm) {
+    FzLayout L;
+    int S, V, threads;
+    int rc = fz_shape(a, L, S, V, threads);
+    if (rc) return rc;
+    FzKernel k = fz_pick(a.material_kind, S, V);
+    cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem_bytes);
+    if (err == cudaSuccess)
+        err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k, threads, L.smem_bytes);
+    if (err != cudaSuccess) {
+        set_error("fdtd_step_occupancy: %s", cudaGetErrorString(err));
+        return FDTD_ERR_CUDA;
+    }
+    return 0;
+}
+
+int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
+    int rc = get_encoder();
+    if (rc) return rc;
+    const int P = a.pitch_z, ty = a.tile_y, RZ = a.psi_rz;
+    FzLayout L;
+    int S, V, nthreads;
+    if ((rc = fz_shape(a, L, S, V, nthreads))) return rc;
     FzMaps maps;
     const cuuint64_t nz = a.nz, ny = a.ny, nx = a.nx, pz = P;
     cuuint64_t fdims[4] = {nz, ny, nx, 3};
@@ -641,25 +703,10 @@ int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
     }
     const int tiles = (a.ny + ty - 1) / ty;
     const int chunks = (a.nx + a.chunk_x - 1) / a.chunk_x;
-    dim3 grid((unsigned)(tiles * chunks));
-    dim3 threads((unsigned)(lanes * (ty + 1)));
-#define LAUNCH3(M, SS, W)                                                                    \
-    do {                                                                                     \
-        cudaFuncSetAttribute(fz_step_kernel<M, SS, W>,                                       \
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem_bytes);      \
-        fz_step_kernel<M, SS, W><<<grid, threads, L.smem_bytes, stream>>>(maps, prm);        \
-    } while (0)
-#define LAUNCH(M, SS)                                                                        \
-    do {                                                                                     \
-        if (V == 4) LAUNCH3(M, SS, 4); else LAUNCH3(M, SS, 2);                                \
-    } while (0)
-    if (a.material_kind == 1) {
-        if (S == 2) LAUNCH(1, 2); else if (S == 3) LAUNCH(1, 3); else LAUNCH(1, 4);
-    } else {
-        if (S == 2) LAUNCH(0, 2); else if (S == 3) LAUNCH(0, 3); else LAUNCH(0, 4);
-    }
-#undef LAUNCH3
-#undef LAUNCH
+    dim3 grid((unsigned)(a.schedule ? a.schedule_blocks : tiles * chunks));
+    FzKernel kern = fz_pick(a.material_kind, S, V);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem_bytes);
+    kern<<<grid, dim3((unsigned)nthreads), L.smem_bytes, stream>>>(maps, prm);
     return launch_status("fdtd_step_fused (full-z TMA)");
 }
 

@@ -22,6 +22,8 @@ TmaLayout tma_layout(int ty, int tz, int stages, int mat);
 bool tma_eligible(const fdtd_step_args &a);
 int launch_tma(const fdtd_step_args &a, cudaStream_t stream);
 bool fz_eligible(const fdtd_step_args &a);
+void fz_defaults(fdtd_step_args &a);
+int fz_occupancy(const fdtd_step_args &a, int *blocks_per_sm);
 int launch_fz(const fdtd_step_args &a, cudaStream_t stream);
 
 }  // namespace wfb

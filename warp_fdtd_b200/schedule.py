@@ -1,0 +1,56 @@
+"""Cost-balanced block schedule of the full-z fused step (path 3).
+
+The full-z kernel gives each block one tile of `tile_y` rows and a run of x
+planes.  Planes cost more where the block also filters CPML state along x or
+y: the x- and y-slab psi are read and written directly, and on a B200 such a
+plane took about 1.5x an interior plane.  A uniform grid of equal chunks
+therefore ends with the CPML blocks running alone.  This module instead cuts
+each tile's x extent into runs of equal estimated cost and hands the runs out
+so that every resident block slot of the GPU gets one run: one wave, no tail.
+
+`balanced_schedule` returns the (blocks, 4) int32 table of
+`fdtd_step_args.schedule`: (y tile index, first plane, end plane, 0).
+"""
+
+import numpy as np
+
+# Extra cost of a plane whose tile holds y-slab rows / whose x position is an
+# x-slab plane, relative to an interior plane (B200, 20 nm bend, tile_y 5).
+Y_WEIGHT = 0.6
+X_WEIGHT = 0.5
+
+
+def plane_costs(shape, tile_y, coeff_e, coeff_h, wy=Y_WEIGHT, wx=X_WEIGHT):
+    """(tiles, nx) estimated cost of each tile plane; coeff_* are the (3, L, 4)
+    CPML tables (a, b, 1/kappa, rank) of E and H."""
+    nx, ny, _ = shape
+    tiles = (ny + tile_y - 1) // tile_y
+    yrow = (coeff_e[1, :ny, 0] != 0) | (coeff_h[1, :ny, 0] != 0)
+    xact = ((coeff_e[0, :nx, 0] != 0) | (coeff_h[0, :nx, 0] != 0)).astype(np.float64)
+    ytile = np.array([yrow[t * tile_y:(t + 1) * tile_y].any() for t in range(tiles)], np.float64)
+    return 1.0 + wy * ytile[:, None] + wx * xact[None, :]
+
+
+def balanced_schedule(shape, tile_y, coeff_e, coeff_h, blocks, wy=Y_WEIGHT, wx=X_WEIGHT):
+    """Split every tile's planes into runs of equal estimated cost, about
+    `blocks` runs in all (at least one per tile)."""
+    cost = plane_costs(shape, tile_y, coeff_e, coeff_h, wy, wx)
+    nx = shape[0]
+    tiles = cost.shape[0]
+    per_tile = cost.sum(axis=1)
+    share = per_tile / per_tile.sum() * max(int(blocks), tiles)
+    runs = np.maximum(1, np.floor(share).astype(np.int64))
+    while runs.sum() < max(int(blocks), tiles):
+        runs[np.argmax(share - runs)] += 1
+    runs = np.minimum(runs, nx)
+    entries = []
+    for t in range(tiles):
+        cum = np.concatenate([[0.0], np.cumsum(cost[t])])
+        cuts = [0]
+        for j in range(1, int(runs[t])):
+            cuts.append(int(np.searchsorted(cum, cum[-1] * j / runs[t])))
+        cuts.append(nx)
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            if b > a:
+                entries.append((t, a, b, 0))
+    return np.asarray(entries, np.int32).reshape(-1, 4)

@@ -15,6 +15,7 @@ the reference `Solver` (solver.py:53-264).  What changes underneath:
 All device memory is torch tensors; every kernel runs through the C ABI.
 """
 
+import ctypes
 import json
 import time
 from pathlib import Path
@@ -24,6 +25,7 @@ import torch
 
 from . import _lib
 from . import kernels as k
+from .schedule import balanced_schedule
 from ._lib import ptr
 from .bundle import read_bundle
 
@@ -145,7 +147,7 @@ SUPPORTED_PROFILES = ("SingleFrequencyProfile", "GaussianPulseProfile", "HannPul
 
 class Solver:
     def __init__(self, case, device="cuda:0", graph_steps=64, cpml_storage="full",
-                 material="auto", tile=None, path=0):
+                 material="auto", tile=None, path=0, schedule="balanced"):
         if cpml_storage not in ("full", "packed"):
             raise ValueError("cpml_storage must be full or packed")
         if material not in ("auto", "u8", "f32"):
@@ -186,6 +188,11 @@ class Solver:
             raise ValueError("graph_steps must be positive")
         self.courant = factor / np.sqrt(3)
         self.tile = tuple(tile) if tile else (0, 0, 0)
+        if schedule not in ("balanced", "uniform"):
+            raise ValueError("schedule must be balanced or uniform")
+        # full-z path: cost-balanced one-wave block schedule, or uniform chunks
+        # (also used whenever a tile sets chunk_x)
+        self.schedule = schedule
         if path not in (0, 1, 2, 3):
             raise ValueError("path must be 0 (auto), 1, 2 or 3")
         self.kernel_path = int(path)
@@ -412,6 +419,24 @@ class Solver:
         a.material_pitch = self._mpitch
         a.tile_y, a.tile_z, a.chunk_x = (int(v) for v in self.tile)
         a.path = int(self.kernel_path)
+        self._schedule = None
+        if self._psi_layout == 2 and self.schedule == "balanced" and a.chunk_x <= 0:
+            # one wave of cost-balanced (tile, x run) blocks, see schedule.py
+            ce = self._coeff_step["E"].cpu().numpy()
+            ch = self._coeff_step["H"].cpu().numpy()
+            slots, runs = None, None
+            for _ in range(3):  # the run length sizes shared memory, hence occupancy
+                blocks, sms = ctypes.c_int(0), ctypes.c_int(0)
+                _lib.call("fdtd_step_occupancy", ctypes.byref(a), ctypes.byref(blocks),
+                          ctypes.byref(sms))
+                if blocks.value * sms.value == slots:
+                    break
+                slots = blocks.value * sms.value
+                runs = balanced_schedule(self.shape, a.tile_y or 5, ce, ch, slots)
+                a.chunk_x = int((runs[:, 2] - runs[:, 1]).max())
+            self._schedule = torch.from_numpy(runs).to(self.device)
+            a.schedule = ptr(self._schedule)
+            a.schedule_blocks = int(runs.shape[0])
         return a
 
     def set_tile(self, tile_y, tile_z, chunk_x=0):
