@@ -184,7 +184,9 @@ __device__ __forceinline__ bool group_ranks_ok(const float4 *tab, int RZ) {
     return !psi || (ok && rb % V == 0 && rb + V <= RZ);
 }
 
-template <int MAT, int S, int V>
+// FULLZ: rows hold no padding (nz == pitch_z), so no cell group needs the
+// z < nz masks; dropping them frees registers the update's schedule uses.
+template <int MAT, int S, int V, bool FULLZ>
 __global__ void __launch_bounds__(512)
     fz_step_kernel(const __grid_constant__ FzMaps maps, const __grid_constant__ FzParams prm) {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -439,13 +441,13 @@ __global__ void __launch_bounds__(512)
                     float v1 = e1.v[j] + (courant * (dz[0].v[j] - dx[2].v[j])) * iej;
                     float v2 = e2.v[j] + (courant * (dx[1].v[j] - dy[0].v[j])) * iej;
                     const int gz = zv + j;
-                    if (p == a.source_x && wave_ok && gz < nz) {
+                    if (p == a.source_x && wave_ok && (FULLZ || gz < nz)) {
                         const i64 sidx = (i64)gy * nz + gz;
                         const i64 syz = (i64)ny * nz;
                         v1 = v1 + ((a.src_h[2 * syz + sidx] * a.waves_h[2 * a.waves_cols + t]) * courant) * iej;
                         v2 = v2 - ((a.src_h[syz + sidx] * a.waves_h[a.waves_cols + t]) * courant) * iej;
                     }
-                    const bool in = gz < nz;
+                    const bool in = FULLZ || gz < nz;
                     o[0].v[j] = in ? v0 : 0.0f;
                     o[1].v[j] = in ? v1 : 0.0f;
                     o[2].v[j] = in ? v2 : 0.0f;
@@ -508,7 +510,7 @@ __global__ void __launch_bounds__(512)
                 float v1 = h1.v[j] - courant * (dz[0].v[j] - dx[2].v[j]);
                 float v2 = h2.v[j] - courant * (dx[1].v[j] - dy[0].v[j]);
                 const int gz = zv + j;
-                if (q == a.source_x && wave_ok && gz < nz) {
+                if (q == a.source_x && wave_ok && (FULLZ || gz < nz)) {
                     const i64 sidx = (i64)gy * nz + gz;
                     const i64 syz = (i64)ny * nz;
                     v1 = v1 - (a.src_e[2 * syz + sidx] * a.waves_e[2 * a.waves_cols + t]) * courant;
@@ -600,13 +602,16 @@ void fz_defaults(fdtd_step_args &a) {
 using FzKernel = void (*)(FzMaps, FzParams);
 
 template <int M, int SS>
-static FzKernel fz_pick_v(int V) {
-    return V == 4 ? fz_step_kernel<M, SS, 4> : fz_step_kernel<M, SS, 2>;
+static FzKernel fz_pick_v(int V, bool full) {
+    if (full) return V == 4 ? fz_step_kernel<M, SS, 4, true> : fz_step_kernel<M, SS, 2, true>;
+    return V == 4 ? fz_step_kernel<M, SS, 4, false> : fz_step_kernel<M, SS, 2, false>;
 }
 
-static FzKernel fz_pick(int mat, int S, int V) {
-    if (mat == 1) return S == 2 ? fz_pick_v<1, 2>(V) : S == 3 ? fz_pick_v<1, 3>(V) : fz_pick_v<1, 4>(V);
-    return S == 2 ? fz_pick_v<0, 2>(V) : S == 3 ? fz_pick_v<0, 3>(V) : fz_pick_v<0, 4>(V);
+static FzKernel fz_pick(const fdtd_step_args &a, int S, int V) {
+    const bool full = a.nz == a.pitch_z;
+    if (a.material_kind == 1)
+        return S == 2 ? fz_pick_v<1, 2>(V, full) : S == 3 ? fz_pick_v<1, 3>(V, full) : fz_pick_v<1, 4>(V, full);
+    return S == 2 ? fz_pick_v<0, 2>(V, full) : S == 3 ? fz_pick_v<0, 3>(V, full) : fz_pick_v<0, 4>(V, full);
 }
 
 // Layout, stage count, z cells per thread and threads per block of a launch.
@@ -634,7 +639,7 @@ int fz_occupancy(const fdtd_step_args &a, int *blocks_per_sm) {
     int S, V, threads;
     int rc = fz_shape(a, L, S, V, threads);
     if (rc) return rc;
-    FzKernel k = fz_pick(a.material_kind, S, V);
+    FzKernel k = fz_pick(a, S, V);
     cudaError_t err = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem_bytes);
     if (err == cudaSuccess)
         err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k, threads, L.smem_bytes);
@@ -704,7 +709,7 @@ int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
     const int tiles = (a.ny + ty - 1) / ty;
     const int chunks = (a.nx + a.chunk_x - 1) / a.chunk_x;
     dim3 grid((unsigned)(a.schedule ? a.schedule_blocks : tiles * chunks));
-    FzKernel kern = fz_pick(a.material_kind, S, V);
+    FzKernel kern = fz_pick(a, S, V);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem_bytes);
     kern<<<grid, dim3((unsigned)nthreads), L.smem_bytes, stream>>>(maps, prm);
     return launch_status("fdtd_step_fused (full-z TMA)");
