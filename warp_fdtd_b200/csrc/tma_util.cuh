@@ -63,11 +63,6 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
         : "memory");
 }
 
-// Pull `bytes` (a multiple of 16) at a 16-byte aligned global address into L2.
-__device__ __forceinline__ void l2_prefetch(const void *ptr, unsigned bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(bytes) : "memory");
-}
-
 inline PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 
 inline int get_encoder() {
