@@ -287,7 +287,7 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = load_peaks()
     traffic = None
     tfile = ROOT / "profiles" / "fused_step_traffic.json"
-    if tfile.exists():
+    if tfile.exists() and args.workload == "bend20":  # the file holds the full bend's figure
         try:
             traffic = json.loads(tfile.read_text()).get("bytes_per_launch")
         except (ValueError, OSError):
