@@ -247,6 +247,11 @@ typedef struct fdtd_step_args {
 
 int fdtd_step_fused(const fdtd_step_args *args, void *stream);
 
+/* Fill the full-z path's launch-shape defaults into *args (tile_y where 0;
+ * chunk_x where 0 and no schedule is set), as fdtd_step_fused would pick
+ * them.  No reference counterpart. */
+int fdtd_step_defaults(fdtd_step_args *args);
+
 /* Resident blocks per SM of the full-z path's kernel for these arguments
  * (after the defaults fdtd_step_fused would pick) and the device's SM count,
  * for sizing a schedule to whole waves.  No reference counterpart. */

@@ -439,6 +439,24 @@ extern "C" int fdtd_step_fused(const fdtd_step_args *args, void *stream) {
     return launch_status("fdtd_step_fused");
 }
 
+extern "C" int fdtd_step_defaults(fdtd_step_args *args) {
+    if (!args) {
+        set_error("fdtd_step_defaults: null argument");
+        return FDTD_ERR_ARG;
+    }
+    fdtd_step_args a = *args;
+    if (a.pitch_z <= 0) a.pitch_z = a.nz;
+    if (a.material_pitch <= 0) a.material_pitch = a.nz;
+    if (a.nx <= 0 || a.ny <= 0 || a.nz <= 0 || a.packed != FDTD_PSI_SLAB || !fz_eligible(a)) {
+        set_error("fdtd_step_defaults: arguments do not select the full-z path");
+        return FDTD_ERR_ARG;
+    }
+    fz_defaults(a);
+    args->tile_y = a.tile_y;
+    if (!args->schedule) args->chunk_x = a.chunk_x;
+    return 0;
+}
+
 extern "C" int fdtd_step_occupancy(const fdtd_step_args *args, int *blocks_per_sm, int *sms) {
     if (!args || !blocks_per_sm || !sms) {
         set_error("fdtd_step_occupancy: null argument");

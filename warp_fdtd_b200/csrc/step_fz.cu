@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(512)
     uint64_t *bars = (uint64_t *)smem;
     int *meta = (int *)(smem + 64);  // [0] slab rank check failed
     unsigned char *stage0 = smem + L.off_stages;
-    float *ring = (float *)(smem + L.off_ring);  // [2][3][TY+1][RW]
+    float *ring = (float *)(smem + L.off_ring);  // [3][TY+1][RW]: E of the last plane
     float4 *cey = (float4 *)(smem + L.off_coef);
     float4 *chy = cey + (TY + 1);
     float4 *cez = chy + (TY + 1);
@@ -291,7 +291,7 @@ __global__ void __launch_bounds__(512)
         chx[j] = p >= 1 && p - 1 < nx ? __ldg(ch + p - 1) : ident;
     }
     // the ring's +z pad columns (z = P .. P+3) are the zero padding beyond the grid
-    for (int j = tid; j < 2 * 3 * (TY + 1) * 4; j += nth) {
+    for (int j = tid; j < 3 * (TY + 1) * 4; j += nth) {
         const int r = j >> 2, c = j & 3;
         ring[r * RW + P + c] = 0.0f;
     }
@@ -378,10 +378,10 @@ __global__ void __launch_bounds__(512)
                 timed_out = true;
         }
         const unsigned char *stc = stage_ptr(k);
-        float *Rc = ring + (k & 1) * 3 * RS;
         // ---------------- E update, rows y0 .. y0+TY ----------------
+        // (kept in registers until the H update below has read plane q's E)
+        VF<V> o[3] = {zero_v<V>(), zero_v<V>(), zero_v<V>()};
         if (!timed_out) {
-            VF<V> o[3] = {zero_v<V>(), zero_v<V>(), zero_v<V>()};
             if (p < nx && row_in) {
                 const float *Hc = (const float *)(stc + L.off_h);
                 const float *Eo = (const float *)(stc + L.off_e);
@@ -459,9 +459,6 @@ __global__ void __launch_bounds__(512)
                     stv<V>(dst + 2 * cols, o[2]);
                 }
             }
-            stv<V>(Rc + r_off, o[0]);
-            stv<V>(Rc + RS + r_off, o[1]);
-            stv<V>(Rc + 2 * RS + r_off, o[2]);
         }
         if (__syncthreads_or(timed_out)) {
             timed_out = true;
@@ -474,12 +471,12 @@ __global__ void __launch_bounds__(512)
         }
         // ---------------- H update at plane q = p - 1, rows y0 .. y0+TY-1 ----------------
         if (h_on) {
-            const float *Rq = ring + ((k - 1) & 1) * 3 * RS;
+            const float *Rq = ring;  // E of plane q
             VF<V> dx[3], dy[3], dz[3];
 #pragma unroll
             for (int r = 0; r < 3; ++r) {
                 const VF<V> eq = ldsv<V>(Rq + r * RS + r_off);
-                const VF<V> ep = ldsv<V>(Rc + r * RS + r_off);
+                const VF<V> &ep = o[r];
                 const VF<V> eyp = ldsv<V>(Rq + r * RS + r_off + RW);
                 const float zp = Rq[r * RS + r_off + V];
 #pragma unroll
@@ -531,6 +528,10 @@ __global__ void __launch_bounds__(512)
             for (int c = 0; c < 3; ++c) hprev[c] = ldsv<V>(Hc + c * HS + h_off);
         }
         __syncthreads();
+        // every H update has read plane q's E: the ring takes plane p's
+        stv<V>(ring + r_off, o[0]);
+        stv<V>(ring + RS + r_off, o[1]);
+        stv<V>(ring + 2 * RS + r_off, o[2]);
     }
     if (timed_out) {
         if (tid == 0) {
@@ -567,7 +568,7 @@ static FzLayout fz_layout(int ty, int P, int RZ, int S, int mat, int chunk_x) {
     L.off_stages = 128;
     L.RW = P + 4;
     L.off_ring = (int)(L.off_stages + (size_t)S * L.stage_bytes);
-    size_t ring = (size_t)2 * 3 * (ty + 1) * L.RW * 4;
+    size_t ring = (size_t)3 * (ty + 1) * L.RW * 4;
     L.off_coef = (int)up(L.off_ring + ring, 16);
     L.XK = chunk_x + 2;  // x coefficients of planes xa-1 .. xb (E) and xa-2 .. xb-1 (H)
     size_t coef = (size_t)(2 * (ty + 1) + 2 * P + 2 * L.XK) * 16;
@@ -588,7 +589,18 @@ bool fz_eligible(const fdtd_step_args &a) {
 }
 
 void fz_defaults(fdtd_step_args &a) {
-    if (a.tile_y <= 0) a.tile_y = 5;
+    if (a.tile_y <= 0) {
+        // the tallest tile whose block keeps two per SM (<= 256 threads at 128
+        // registers, <= 112 KB with a three-stage ring and 40-plane runs)
+        const int V = a.vector == 2 ? 2 : 4, lanes = a.pitch_z / V;
+        a.tile_y = 1;
+        for (int ty = 256 / lanes - 1; ty >= 1; --ty)
+            if (fz_layout(ty, a.pitch_z, a.psi_rz, a.stages > 0 ? a.stages : 3, a.material_kind, 40)
+                    .smem_bytes <= 112 * 1024) {
+                a.tile_y = ty;
+                break;
+            }
+    }
     if (a.chunk_x <= 0 && !a.schedule) {
         // about three waves of two resident blocks per SM, chunks of >= 16 planes
         const int tiles = (a.ny + a.tile_y - 1) / a.tile_y;

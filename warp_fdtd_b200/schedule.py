@@ -15,8 +15,8 @@ so that every resident block slot of the GPU gets one run: one wave, no tail.
 import numpy as np
 
 # Extra cost of a plane whose tile holds y-slab rows / whose x position is an
-# x-slab plane, relative to an interior plane (B200, 20 nm bend, tile_y 5: the
-# best of a sweep over 0.6..1.5 / 0.5..1.3).
+# x-slab plane, relative to an interior plane (B200, 20 nm bend: the best of
+# sweeps over 0.6..1.5 / 0.5..1.3 at tile_y 5 and 6).
 Y_WEIGHT = 0.9
 X_WEIGHT = 0.7
 

@@ -188,6 +188,7 @@ class Solver:
             raise ValueError("graph_steps must be positive")
         self.courant = factor / np.sqrt(3)
         self.tile = tuple(tile) if tile else (0, 0, 0)
+        self.stages = 0
         if schedule not in ("balanced", "uniform"):
             raise ValueError("schedule must be balanced or uniform")
         # full-z path: cost-balanced one-wave block schedule, or uniform chunks
@@ -418,10 +419,12 @@ class Solver:
         a.pitch_z = self._pitch
         a.material_pitch = self._mpitch
         a.tile_y, a.tile_z, a.chunk_x = (int(v) for v in self.tile)
+        a.stages = self.stages
         a.path = int(self.kernel_path)
         self._schedule = None
         if self._psi_layout == 2 and self.schedule == "balanced" and a.chunk_x <= 0:
             # one wave of cost-balanced (tile, x run) blocks, see schedule.py
+            _lib.call("fdtd_step_defaults", ctypes.byref(a))  # the tile height
             ce = self._coeff_step["E"].cpu().numpy()
             ch = self._coeff_step["H"].cpu().numpy()
             slots, runs = None, None
@@ -432,16 +435,19 @@ class Solver:
                 if blocks.value * sms.value == slots:
                     break
                 slots = blocks.value * sms.value
-                runs = balanced_schedule(self.shape, a.tile_y or 5, ce, ch, slots)
+                runs = balanced_schedule(self.shape, a.tile_y, ce, ch, slots)
                 a.chunk_x = int((runs[:, 2] - runs[:, 1]).max())
             self._schedule = torch.from_numpy(runs).to(self.device)
             a.schedule = ptr(self._schedule)
             a.schedule_blocks = int(runs.shape[0])
         return a
 
-    def set_tile(self, tile_y, tile_z, chunk_x=0):
-        """Change the fused kernel's launch shape; captured graphs are dropped."""
+    def set_tile(self, tile_y, tile_z, chunk_x=0, stages=0):
+        """Change the fused kernel's launch shape (tile rows, tile z cells,
+        planes per block with 0 for the schedule, TMA ring stages with 0 for the
+        default); captured graphs are dropped."""
         self.tile = (int(tile_y), int(tile_z), int(chunk_x))
+        self.stages = int(stages)
         self._args = self._step_args()
         self.graphs = {}
 
