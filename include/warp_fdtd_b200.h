@@ -272,6 +272,19 @@ int fdtd_record_phasor64(const float *E0, const float *E1, const float *H0, cons
                          int nz, int pitch_z, int x0, int y0, int z0, int sx, int sy, int sz,
                          int exact, void *stream);
 
+/* Volume phasor observer (volume.py:60-89, record_volume) with float64
+ * accumulators.  With t = step[0] and the buffer convention of
+ * fdtd_record_phasor64, if first <= t < nsteps every sampling point i
+ * (positions (count, 3) float32, grid units: position / spacing from the
+ * grid's lower corner) gets phasor[c, i] (re, im) += weights[t] * f_c, where
+ * f_c is component c trilinearly interpolated (zero outside the grid) at the
+ * point minus the component's Yee offset, and H is the mean of H(n+1/2) and
+ * H(n-1/2).  weights (nsteps, 2) float32; phasor (6, count, 2) float64. */
+int fdtd_record_volume(const float *E0, const float *E1, const float *H0, const float *H1,
+                       const int *step, const float *positions, long long count,
+                       const float *weights, int nsteps, int first, double *phasor, int nx,
+                       int ny, int nz, int pitch_z, void *stream);
+
 /* Flux branch of detectors.py:104-106 with float64 bins, same buffer
  * convention as fdtd_record_phasor64: if t < nsteps and 0 <= indices[t] <
  * nbins, flux[indices[t]] += sum over the plane of cross(E, H)[axis] * area

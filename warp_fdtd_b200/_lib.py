@@ -75,6 +75,7 @@ _SIGNATURES = {
     "fdtd_advance": [_p, _i, _p],
     "fdtd_step_occupancy": [ctypes.POINTER(StepArgs), _p, _p],
     "fdtd_step_defaults": [ctypes.POINTER(StepArgs)],
+    "fdtd_record_volume": [_p, _p, _p, _p, _p, _p, _ll, _p, _i, _i, _p, _i, _i, _i, _i, _p],
     "fdtd_record": [_p, _p, _p, _ll, _p, _p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i,
                     _i, _i, _i, _i, _p],
     "fdtd_record_curl": [_p, _ll, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i, _f, _p],

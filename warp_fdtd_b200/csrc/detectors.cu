@@ -118,6 +118,72 @@ __global__ void record_stage_kernel(const float *__restrict__ E0, const float *_
     }
 }
 
+// volume.py:24-41: component `comp` of f trilinearly interpolated at grid
+// position (px, py, pz); taps outside the grid count as zero.  Same float32
+// operation order as the reference.
+__device__ __forceinline__ float trilinear(const float *__restrict__ f, i64 n, int comp, float px,
+                                           float py, float pz, int nx, int ny, int nz,
+                                           int pitch) {
+    const int ix = (int)floorf(px), iy = (int)floorf(py), iz = (int)floorf(pz);
+    const float tx = px - (float)ix, ty = py - (float)iy, tz = pz - (float)iz;
+    float value = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int x = ix + a, y = iy + b, z = iz + c;
+                if (x >= 0 && y >= 0 && z >= 0 && x < nx && y < ny && z < nz) {
+                    const float w = ((a ? tx : 1.0f - tx) * (b ? ty : 1.0f - ty)) * (c ? tz : 1.0f - tz);
+                    value = value + w * f[comp * n + ((i64)x * ny + y) * pitch + z];
+                }
+            }
+    return value;
+}
+
+// volume.py:60-89 with float64 accumulators: one thread per sampling point;
+// component c is sampled at the point minus its Yee offset, H as the mean of
+// H(n+1/2) and H(n-1/2).
+__global__ void record_volume_kernel(const float *__restrict__ E0, const float *__restrict__ E1,
+                                     const float *__restrict__ H0, const float *__restrict__ H1,
+                                     const int *__restrict__ step,
+                                     const float *__restrict__ positions, i64 count,
+                                     const float2 *__restrict__ weights, int nsteps, int first,
+                                     double2 *__restrict__ phasor, int nx, int ny, int nz,
+                                     int pitch) {
+    const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int t = step[0];
+    if (t < first || t < 0 || t >= nsteps) return;
+    const float2 w = weights[t];
+    const int s = t & 1;
+    const float *e = s ? E0 : E1;
+    const float *h = s ? H0 : H1;
+    const float *prev = s ? H1 : H0;
+    const i64 n = (i64)nx * ny * pitch;
+    const float px = positions[3 * i], py = positions[3 * i + 1], pz = positions[3 * i + 2];
+    // Yee offsets of Ex, Ey, Ez, Hx, Hy, Hz (volume.py:44-57)
+    const float ox[6] = {0.5f, 0.0f, 0.0f, 0.0f, 0.5f, 0.5f};
+    const float oy[6] = {0.0f, 0.5f, 0.0f, 0.5f, 0.0f, 0.5f};
+    const float oz[6] = {0.0f, 0.0f, 0.5f, 0.5f, 0.5f, 0.0f};
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+        const float qx = px - ox[c], qy = py - oy[c], qz = pz - oz[c];
+        float value;
+        if (c < 3)
+            value = trilinear(e, n, c, qx, qy, qz, nx, ny, nz, pitch);
+        else
+            value = 0.5f * (trilinear(h, n, c - 3, qx, qy, qz, nx, ny, nz, pitch) +
+                            trilinear(prev, n, c - 3, qx, qy, qz, nx, ny, nz, pitch));
+        double2 *p = phasor + (i64)c * count + i;
+        double2 acc = *p;
+        acc.x = acc.x + (double)w.x * (double)value;
+        acc.y = acc.y + (double)w.y * (double)value;
+        *p = acc;
+    }
+}
+
 // One thread per (component, cell); the window's weights are staged in
 // shared memory ([k][t] float2).
 __global__ void dft_fold_kernel(const int *__restrict__ step, const int *__restrict__ indices,
@@ -238,6 +304,22 @@ int fdtd_dft_fold(const int *step, const int *indices, int nsteps, const float *
         step, indices, nsteps, (const float2 *)weights, nfreq, stage, T, (double2 *)phasor,
         count);
     return launch_status("fdtd_dft_fold");
+}
+
+int fdtd_record_volume(const float *E0, const float *E1, const float *H0, const float *H1,
+                       const int *step, const float *positions, long long count,
+                       const float *weights, int nsteps, int first, double *phasor, int nx,
+                       int ny, int nz, int pitch_z, void *stream) {
+    if (pitch_z <= 0) pitch_z = nz;
+    if (count <= 0 || nsteps < 1 || nx < 1 || ny < 1 || nz < 1 || pitch_z < nz || !E0 || !E1 ||
+        !H0 || !H1 || !step || !positions || !weights || !phasor) {
+        set_error("fdtd_record_volume: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    record_volume_kernel<<<(unsigned)((count + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        E0, E1, H0, H1, step, positions, (i64)count, (const float2 *)weights, nsteps, first,
+        (double2 *)phasor, nx, ny, nz, pitch_z);
+    return launch_status("fdtd_record_volume");
 }
 
 }  // extern "C"

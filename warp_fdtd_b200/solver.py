@@ -25,7 +25,7 @@ import torch
 
 from . import _lib
 from . import kernels as k
-from .schedule import balanced_schedule
+from .schedule import X_WEIGHT, Y_WEIGHT, balanced_schedule
 from ._lib import ptr
 from .bundle import read_bundle
 
@@ -194,6 +194,7 @@ class Solver:
         # full-z path: cost-balanced one-wave block schedule, or uniform chunks
         # (also used whenever a tile sets chunk_x)
         self.schedule = schedule
+        self.schedule_weights = (Y_WEIGHT, X_WEIGHT)
         if path not in (0, 1, 2, 3):
             raise ValueError("path must be 0 (auto), 1, 2 or 3")
         self.kernel_path = int(path)
@@ -435,12 +436,59 @@ class Solver:
                 if blocks.value * sms.value == slots:
                     break
                 slots = blocks.value * sms.value
-                runs = balanced_schedule(self.shape, a.tile_y, ce, ch, slots)
+                runs = balanced_schedule(self.shape, a.tile_y, ce, ch, slots,
+                                         *self.schedule_weights)
                 a.chunk_x = int((runs[:, 2] - runs[:, 1]).max())
             self._schedule = torch.from_numpy(runs).to(self.device)
             a.schedule = ptr(self._schedule)
             a.schedule_blocks = int(runs.shape[0])
         return a
+
+    def autotune(self, tiles=None, stages=(3, 2), weights=None, repeats=20):
+        """Pick the fused step's launch shape by timing it on this grid.
+
+        Every candidate (tile rows, TMA stages, schedule cost weights) is timed
+        over `repeats` fused steps with CUDA events after a warm-up; the
+        fastest is kept.  Candidates that do not fit (shared memory, threads)
+        are skipped.  The solver is reset afterwards.  Returns the timings
+        {(tile_y, stages, weights): ms}.  Only the full-z path is tuned."""
+        if self._psi_layout != 2:
+            raise ValueError("autotune tunes the full-z path (path 0 or 3)")
+        a = self._step_args()
+        _lib.call("fdtd_step_defaults", ctypes.byref(a))
+        base = int(a.tile_y)
+        tiles = tiles or sorted({max(1, base - 1), base, base + 1})
+        weights = weights or [self.schedule_weights, (0.6, 0.5), (1.2, 1.0)]
+        stream = torch.cuda.current_stream(self.device)
+        saved = (self.tile, self.stages, self.schedule_weights)
+        timings = {}
+        for ty in tiles:
+            for st in stages:
+                for w in weights:
+                    self.schedule_weights = tuple(w)
+                    try:
+                        self.set_tile(ty, 0, 0, st)
+                        for _ in range(3):
+                            _lib.call("fdtd_step_fused", self._args, stream.cuda_stream)
+                    except (ValueError, _lib.FdtdError):
+                        continue
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    for _ in range(repeats):
+                        _lib.call("fdtd_step_fused", self._args, stream.cuda_stream)
+                    e1.record(stream)
+                    e1.synchronize()
+                    timings[(ty, st, tuple(w))] = e0.elapsed_time(e1) / repeats
+        if timings:
+            ty, st, w = min(timings, key=timings.get)
+            self.schedule_weights = w
+            self.set_tile(ty, 0, 0, st)
+        else:
+            self.tile, self.stages, self.schedule_weights = saved
+            self.set_tile(self.tile[0], self.tile[1], self.tile[2], self.stages)
+        self.reset()
+        return timings
 
     def set_tile(self, tile_y, tile_z, chunk_x=0, stages=0):
         """Change the fused kernel's launch shape (tile rows, tile z cells,
