@@ -13,14 +13,14 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "build" / "liboracle.so"
 
-_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _i64 = ctypes.c_longlong
 _int = ctypes.c_int
-_flt = ctypes.c_float
 
-_lib = None
+LIB64_PATH = HERE / "build" / "liboracle64.so"
+
+_libs = {}
 
 
 def build():
@@ -28,55 +28,63 @@ def build():
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not LIB_PATH.exists():
+def lib(f64=False):
+    """The float32 restatement, or with f64 the same compiled in double
+    (every float argument then float64 / c_double)."""
+    if f64 not in _libs:
+        path = LIB64_PATH if f64 else LIB_PATH
+        if not path.exists():
             build()
-        L = ctypes.CDLL(str(LIB_PATH))
-        L.oracle_update.argtypes = [
-            _int, _int, _f32p, _f32p, _i64, _f32p, _f32p, _i64, _f32p, _int,
-            _f32p, _i64, _f32p, _i64, _i32p, _f32p, _i64, _int, _int, _int, _int,
-            _int, _flt, _int,
-        ]
-        L.oracle_record_phasor.argtypes = [
-            _f32p, _f32p, _f32p, _i64, _int, _f32p, _int, _i64, _f64p,
-            _int, _int, _int, _int, _int, _int, _int, _int, _int, _int,
-        ]
-        L.oracle_record_phasor_f32.argtypes = [
-            _f32p, _f32p, _f32p, _i64, _int, _f32p, _f32p,
-            _int, _int, _int, _int, _int, _int, _int, _int, _int, _int,
-        ]
-        L.oracle_flux_sum.argtypes = [
-            _f32p, _f32p, _f32p, _i64, _f32p, _int, _int, _int, _int, _int, _int,
-            _int, _int, _int, _int, _int,
-        ]
-        L.oracle_flux_sum.restype = ctypes.c_double
-        L.oracle_record_curl.argtypes = [
-            _f32p, _i64, _f32p, _i64, _int, _int, _int, _int, _int, _int, _int,
-            _int, _int, _int, _flt,
-        ]
-        L.oracle_prepare.argtypes = [
-            _f32p, _f32p, _f32p, _f32p, _int, _f32p, _int, _int, _int, _flt, _int,
-        ]
-        L.oracle_gather.argtypes = [
-            _f32p, _f32p, _f32p, _i64, ctypes.c_void_p, _int, _int, _int, _int, _int,
-            _int, _int, _int, _int, _int, _int, _int,
-        ]
-        L.oracle_inject.argtypes = [
-            _f32p, _f32p, _f32p, _f32p, _int, _int, _int, _int, _int, _int, _int,
-            _int, _int, _int, _int,
-        ]
-        L.oracle_write_design.argtypes = [
-            _f32p, _f32p, _int, _int, _int, _int, _int, _int, _int, _int, _int,
-        ]
-        L.oracle_run_steps.argtypes = [
-            _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _int, _f32p, _f32p,
-            _f32p, _f32p, _i64, _int, _int, _int, _int, _int, _int, _flt,
-        ]
-        L.oracle_num_threads.restype = _int
-        _lib = L
-    return _lib
+        _libs[f64] = _load(path, f64)
+    return _libs[f64]
+
+
+def _load(path, f64):
+    _rp = np.ctypeslib.ndpointer(np.float64 if f64 else np.float32, flags="C_CONTIGUOUS")
+    _rs = ctypes.c_double if f64 else ctypes.c_float
+    L = ctypes.CDLL(str(path))
+    L.oracle_update.argtypes = [
+        _int, _int, _rp, _rp, _i64, _rp, _rp, _i64, _rp, _int,
+        _rp, _i64, _rp, _i64, _i32p, _rp, _i64, _int, _int, _int, _int,
+        _int, _rs, _int,
+    ]
+    L.oracle_record_phasor.argtypes = [
+        _rp, _rp, _rp, _i64, _int, _rp, _int, _i64, _f64p,
+        _int, _int, _int, _int, _int, _int, _int, _int, _int, _int,
+    ]
+    L.oracle_record_phasor_f32.argtypes = [
+        _rp, _rp, _rp, _i64, _int, _rp, _rp,
+        _int, _int, _int, _int, _int, _int, _int, _int, _int, _int,
+    ]
+    L.oracle_flux_sum.argtypes = [
+        _rp, _rp, _rp, _i64, _rp, _int, _int, _int, _int, _int, _int,
+        _int, _int, _int, _int, _int,
+    ]
+    L.oracle_flux_sum.restype = ctypes.c_double
+    L.oracle_record_curl.argtypes = [
+        _rp, _i64, _rp, _i64, _int, _int, _int, _int, _int, _int, _int,
+        _int, _int, _int, _rs,
+    ]
+    L.oracle_prepare.argtypes = [
+        _rp, _rp, _rp, _rp, _int, _rp, _int, _int, _int, _rs, _int,
+    ]
+    L.oracle_gather.argtypes = [
+        _rp, _rp, _rp, _i64, ctypes.c_void_p, _int, _int, _int, _int, _int,
+        _int, _int, _int, _int, _int, _int, _int,
+    ]
+    L.oracle_inject.argtypes = [
+        _rp, _rp, _rp, _rp, _int, _int, _int, _int, _int, _int, _int,
+        _int, _int, _int, _int,
+    ]
+    L.oracle_write_design.argtypes = [
+        _rp, _rp, _int, _int, _int, _int, _int, _int, _int, _int, _int,
+    ]
+    L.oracle_run_steps.argtypes = [
+        _rp, _rp, _rp, _rp, _rp, _rp, _rp, _int, _rp, _rp,
+        _rp, _rp, _i64, _int, _int, _int, _int, _int, _int, _rs,
+    ]
+    L.oracle_num_threads.restype = _int
+    return L
 
 
 def f32(a):
@@ -90,7 +98,7 @@ def update(electric, f, g, inv_eps, psi, coeff, source, waves, step, hprev,
     Arrays must already be C-contiguous float32 (int32 for step)."""
     nx, ny, nz = shape
     packed = int(coeff.shape[-1] == 4)
-    lib().oracle_update(
+    lib(f.dtype == np.float64).oracle_update(
         int(electric), packed, f, g, f.shape[1], inv_eps, psi, psi.shape[1],
         coeff, coeff.shape[1], source, source.shape[1], waves, waves.shape[1],
         step, hprev, hprev.shape[1], int(save_h_from), nx, ny, nz, int(source_x),

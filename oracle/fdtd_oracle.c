@@ -26,6 +26,14 @@
 #include <omp.h>
 #endif
 
+/* liboracle64.so is this file compiled with -DORACLE_F64: every float of the
+ * restatement (fields, coefficients, psi, weights, scalars) becomes double,
+ * the float64 run the float32 path's rounding error is measured against.
+ * (The f-suffixed literals are exact in both.) */
+#ifdef ORACLE_F64
+#define float double
+#endif
+
 typedef long long i64;
 
 /* kernels.py:8-26 `sample`: three components at (x, y, z), zero outside the

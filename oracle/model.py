@@ -170,7 +170,7 @@ class OracleMonitor:
         if index < 0:
             return
         nx, ny, nz = s.shape
-        L = cpu.lib()
+        L = cpu.lib(s.dtype == np.float64)
         if self.is_phasor:
             L.oracle_record_phasor(
                 s.E, s.H, prev, s.n, int(t), self.weights, self.weights.shape[0],
@@ -205,7 +205,9 @@ class OracleMonitor:
 class OracleSolver:
     """Host-side restatement of solver.py's Solver for a CPU run."""
 
-    def __init__(self, case, cpml_storage="full"):
+    def __init__(self, case, cpml_storage="full", dtype=np.float32):
+        """dtype float64 runs the same restatement in double (liboracle64):
+        the inputs are the float32 run's, widened."""
         self.meta, self.data = load_bundle(case)
         m, d = self.meta, self.data
         eps = d["inv_permittivity"]
@@ -238,12 +240,23 @@ class OracleSolver:
         self.waves = {f: source_waves(m, d, self.steps, f) for f in "EH"}
         self.monitors = []
         self.save_h_from = self.steps
+        self.dtype = np.dtype(dtype)
+        if self.dtype == np.float64:
+            wide = lambda a: np.ascontiguousarray(a, np.float64)
+            self.eps, self.E, self.H, self.hprev = map(wide, (self.eps, self.E, self.H, self.hprev))
+            self.psi_e, self.psi_h = wide(self.psi_e), wide(self.psi_h)
+            self.coeffs = {f: wide(c) for f, c in self.coeffs.items()}
+            self.sources = {f: wide(a) for f, a in self.sources.items()}
+            self.waves = {f: wide(a) for f, a in self.waves.items()}
 
     def attach(self):
         """detectors.py:214-220."""
         for obj in self.meta["objects"]:
             if obj["class"].endswith("Detector"):
                 mon = OracleMonitor(self, obj)
+                if self.dtype == np.float64:
+                    mon.weights = np.ascontiguousarray(mon.weights, np.float64)
+                    mon.area_flat = np.ascontiguousarray(mon.area_flat, np.float64)
                 self.monitors.append(mon)
                 if mon.exact:
                     self.save_h_from = min(self.save_h_from, mon.first)

@@ -198,3 +198,26 @@ def test_mode_solver_effective_index():
     assert 2.3 < n_eff < 2.9
     s = np.sum(np.cross(E.astype(float), H.astype(float), axis=0)[0])
     assert abs(s - 2.0) < 1e-4
+
+
+def test_float32_error_against_a_float64_run(oracle50):
+    """The float32 path's rounding error, stated against the same restatement
+    run in double (liboracle64) on the forward50 bundle (2098 steps): the
+    CUDA path is bitwise equal to the float32 oracle, so these are its errors
+    too.  Measured: E rel-L2 1.09e-6, H 9.5e-7, flux traces 2.8e-8 (input) /
+    5.9e-7 (output); the reference's Warp float32 run sits at the same distance
+    (1.08e-6 / 9.4e-7)."""
+    from oracle.model import OracleSolver
+
+    o64 = OracleSolver(GOLDEN / "forward50_gpu", dtype=np.float64).attach()
+    o64.run()
+    f32, f64 = oracle50.fields(), o64.fields()
+    warp = np.load(GOLDEN / "forward50_gpu" / "warp_fields.npz")
+    for name in ("E", "H"):
+        err, werr = rel(f32[name], f64[name]), rel(warp[name], f64[name])
+        print(f"{name}: float32 vs float64 rel-L2 {err:.3e}, Warp vs float64 {werr:.3e}")
+        assert err < 1e-5 and werr < 1e-5
+    for m32, m64 in zip(oracle50.monitors, o64.monitors):
+        err = rel(m32.flux, m64.flux)
+        print(f"flux {m32.name}: float32 vs float64 rel-L2 {err:.3e}")
+        assert err < 1e-5
