@@ -73,6 +73,7 @@ def build(force=False, verbose=False, ptxas_info=False):
         force
         or not LIB.exists()
         or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs)
+        or LIB.stat().st_mtime < CSRC.stat().st_mtime  # a source added or removed
     ):
         tmp = LIB.with_suffix(".so.tmp")
         cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", *map(str, objs), "-o", str(tmp)]
