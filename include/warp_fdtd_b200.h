@@ -247,6 +247,34 @@ typedef struct fdtd_step_args {
 
 int fdtd_step_fused(const fdtd_step_args *args, void *stream);
 
+/* Batches: many grids advanced by one launch of the full-z step.
+ * fdtd_batch_prepare builds every grid's tensor maps and parameters (each
+ * args[i] as for fdtd_step_fused with the slab psi layout, tile_y and chunk_x
+ * set and equal across the batch, as are the row pitch, z slab width,
+ * material kind and stages; schedule ignored) into `workspace` (device
+ * memory of fdtd_batch_workspace_bytes(count) bytes, 64-byte aligned,
+ * written synchronously: call it outside stream capture) and fills *plan.
+ * fdtd_step_batch then runs one step of every grid with `blocks` blocks,
+ * block b taking the int4 schedule entry b = (grid, y tile, first plane, end
+ * plane) in device memory; each grid's own step[0] selects its parity, and
+ * fdtd_advance_many advances the counters (steps: device array of `count`
+ * device pointers).  Grid parameters live in a device-wide table of 128
+ * slots shared by all live batches: fdtd_batch_release frees a batch's.  No
+ * reference counterpart. */
+typedef struct fdtd_batch_plan {
+    int count, smem_bytes, threads, material_kind, stages, vector, full_rows;
+    int base, device;  /* the batch's parameter slots (at most 128 grids live per device) */
+} fdtd_batch_plan;
+
+long long fdtd_batch_workspace_bytes(int count);
+int fdtd_batch_prepare(const fdtd_step_args *args, int count, void *workspace,
+                       long long workspace_bytes, fdtd_batch_plan *plan);
+int fdtd_step_batch(const fdtd_batch_plan *plan, const void *workspace, const int *schedule,
+                    int blocks, void *stream);
+int fdtd_advance_many(int *const *steps, int count, int delta, void *stream);
+/* Free a prepared batch's parameter slots (the workspace is the caller's). */
+int fdtd_batch_release(fdtd_batch_plan *plan);
+
 /* Fill the full-z path's launch-shape defaults into *args (tile_y where 0;
  * chunk_x where 0 and no schedule is set), as fdtd_step_fused would pick
  * them.  No reference counterpart. */

@@ -38,7 +38,8 @@ def test_batch_of_uneven_instances_matches_single_runs(tmp_path):
         s = Solver(c, graph_steps=8)
         attach(s)
         solvers.append(s)
-    batch = BatchSolver(solvers)
+    batch = BatchSolver(solvers, fused=False)  # uneven z: per-instance streams
+    assert not batch.fused
     batch.compile()
     batch.run()
     for s, (fields, meas) in zip(solvers, alone):
@@ -72,3 +73,36 @@ def test_autotune_keeps_the_fastest_shape_and_parity(tmp_path):
     f, of = s.fields(), o.fields()
     np.testing.assert_array_equal(f["E"], of["E"])
     np.testing.assert_array_equal(f["H"], of["H"])
+
+
+def test_fused_batch_of_uneven_instances_matches_single_runs(tmp_path):
+    """One batched launch per step over grids of different x/y extents (same z
+    pitch and slab width) equals each grid run alone, bit for bit."""
+    from tests.bundles import make_bundle
+    from warp_fdtd_b200.batch import BatchSolver
+    from warp_fdtd_b200.detectors import attach
+    from warp_fdtd_b200.solver import Solver
+
+    cases = [make_bundle(tmp_path / f"f{i}", shape, 26, seed=10 + i)
+             for i, shape in enumerate([(14, 12, 28), (23, 9, 28), (11, 17, 28), (30, 21, 28)])]
+    alone = [_run_alone(c) for c in cases]
+    solvers = []
+    for c in cases:
+        s = Solver(c, graph_steps=8)
+        attach(s)
+        solvers.append(s)
+    batch = BatchSolver(solvers, fused=True)
+    assert batch.fused
+    batch.compile()
+    batch.run()
+    for s, (fields, meas) in zip(solvers, alone):
+        got = s.fields()
+        for name in ("E", "H"):
+            np.testing.assert_array_equal(got[name], fields[name])
+        m = _detectors(s)
+        for key in meas:
+            for got_a, want_a in zip(m[key], meas[key]):
+                np.testing.assert_array_equal(got_a, want_a)
+    batch.reset()
+    batch.run()
+    np.testing.assert_array_equal(solvers[3].fields()["H"], alone[3][0]["H"])

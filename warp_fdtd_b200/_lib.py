@@ -68,6 +68,13 @@ class StepArgs(ctypes.Structure):
     ]
 
 
+class BatchPlan(ctypes.Structure):
+    """Mirror of `fdtd_batch_plan`."""
+
+    _fields_ = [(name, _i) for name in ("count", "smem_bytes", "threads", "material_kind",
+                                        "stages", "vector", "full_rows", "base", "device")]
+
+
 # name -> argtypes (all return int status)
 _SIGNATURES = {
     "fdtd_update": [_i, _i, _p, _p, _ll, _p, _p, _ll, _p, _i, _p, _ll, _p, _ll, _p, _p, _ll,
@@ -75,6 +82,10 @@ _SIGNATURES = {
     "fdtd_advance": [_p, _i, _p],
     "fdtd_step_occupancy": [ctypes.POINTER(StepArgs), _p, _p],
     "fdtd_step_defaults": [ctypes.POINTER(StepArgs)],
+    "fdtd_batch_prepare": [ctypes.POINTER(StepArgs), _i, _p, _ll, ctypes.POINTER(BatchPlan)],
+    "fdtd_step_batch": [ctypes.POINTER(BatchPlan), _p, _p, _i, _p],
+    "fdtd_advance_many": [_p, _i, _i, _p],
+    "fdtd_batch_release": [ctypes.POINTER(BatchPlan)],
     "fdtd_record_volume": [_p, _p, _p, _p, _p, _p, _ll, _p, _i, _i, _p, _i, _i, _i, _i, _p],
     "fdtd_record": [_p, _p, _p, _ll, _p, _p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i,
                     _i, _i, _i, _i, _p],
@@ -126,6 +137,8 @@ def load():
         lib.fdtd_last_error.restype = ctypes.c_char_p
         lib.fdtd_last_error.argtypes = []
         lib.fdtd_version.restype = _i
+        lib.fdtd_batch_workspace_bytes.argtypes = [_i]
+        lib.fdtd_batch_workspace_bytes.restype = _ll
         _lib = lib
     return _lib
 

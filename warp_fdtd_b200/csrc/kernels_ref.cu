@@ -138,6 +138,12 @@ __global__ void update_kernel(float *__restrict__ f, const float *__restrict__ g
 
 __global__ void advance_kernel(int *step, int delta) { step[0] += delta; }
 
+// The step counters of many grids, one thread each.
+__global__ void advance_many_kernel(int *const *steps, int count, int delta) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) steps[i][0] += delta;
+}
+
 // detectors.py:65-106 `record` (float32 phasor, float32 atomic flux).
 __global__ void record_kernel(const float *__restrict__ e, const float *__restrict__ h,
                               const float *__restrict__ prev, i64 cols,
@@ -435,6 +441,15 @@ int fdtd_advance(int *step, int delta, void *stream) {
     }
     advance_kernel<<<1, 1, 0, as_stream(stream)>>>(step, delta);
     return launch_status("fdtd_advance");
+}
+
+int fdtd_advance_many(int *const *steps, int count, int delta, void *stream) {
+    if (!steps || count < 1) {
+        set_error("fdtd_advance_many: null steps or count < 1");
+        return FDTD_ERR_ARG;
+    }
+    advance_many_kernel<<<(count + 127) / 128, 128, 0, as_stream(stream)>>>(steps, count, delta);
+    return launch_status("fdtd_advance_many");
 }
 
 int fdtd_record(const float *e, const float *h, const float *prev, long long cols,

@@ -20,6 +20,9 @@
 // group takes the CPML branch is decided per thread from tile coefficient
 // tables in shared memory.  Outside the slabs the reference's 1 * d == d, so
 // the plain difference is used, bit for bit identical.
+#include <mutex>
+#include <new>
+
 #include "common.cuh"
 #include "step_internal.h"
 #include "tma_util.cuh"
@@ -186,9 +189,12 @@ __device__ __forceinline__ bool group_ranks_ok(const float4 *tab, int RZ) {
 
 // FULLZ: rows hold no padding (nz == pitch_z), so no cell group needs the
 // z < nz masks; dropping them frees registers the update's schedule uses.
+// Body of one block: tile `tyi` over planes [xa, xb) of one grid.  `maps` and
+// `prm` are the kernel parameters of a single-grid launch, or one entry of a
+// batch's instance table in global memory.
 template <int MAT, int S, int V, bool FULLZ>
-__global__ void __launch_bounds__(512)
-    fz_step_kernel(const __grid_constant__ FzMaps maps, const __grid_constant__ FzParams prm) {
+__device__ __forceinline__ void fz_run(const FzMaps &maps, const FzParams &prm, int tyi, int xa,
+                                       int xb) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const fdtd_step_args &a = prm.a;
     const FzLayout &L = prm.L;
@@ -213,24 +219,6 @@ __global__ void __launch_bounds__(512)
     float4 *chx = cex + L.XK;  // ... H coefficient of plane xa-2+k
     float *mtab = (float *)(smem + L.off_mtab);
 
-    const int tiles_y = (ny + TY - 1) / TY;
-    int tyi, xa, xb;
-    if (a.schedule) {
-        // one (y tile, x range) entry per block; reject entries outside the grid
-        // or longer than the chunk the shared-memory layout was sized for
-        const int4 seg = ((const int4 *)a.schedule)[blockIdx.x];
-        tyi = seg.x;
-        xa = seg.y;
-        xb = seg.z;
-        if (tyi < 0 || tyi >= tiles_y || xa < 0 || xb > nx || xb - xa > a.chunk_x) {
-            if (threadIdx.x == 0 && a.error) atomicExch(a.error, 3);
-            return;
-        }
-    } else {
-        tyi = blockIdx.x % tiles_y;
-        xa = (blockIdx.x / tiles_y) * a.chunk_x;
-        xb = min(xa + a.chunk_x, nx);
-    }
     if (xa >= xb) return;
     const int y0 = tyi * TY;
     const int last = xb - xa + 1;  // planes k = 0..last are xa-1 .. xb
@@ -543,6 +531,68 @@ __global__ void __launch_bounds__(512)
     }
 }
 
+// A block's (tile, plane range) from a schedule entry (tile, first plane, end
+// plane) or the uniform tile x chunk grid; false (and error 3) for an entry
+// outside the grid or longer than the shared-memory layout's chunk.
+__device__ __forceinline__ bool fz_block_range(const fdtd_step_args &a, int ty, const int *entry,
+                                               int &tyi, int &xa, int &xb) {
+    const int tiles_y = (a.ny + ty - 1) / ty;
+    if (entry) {
+        tyi = entry[0];
+        xa = entry[1];
+        xb = entry[2];
+        if (tyi < 0 || tyi >= tiles_y || xa < 0 || xb > a.nx || xb - xa > a.chunk_x) {
+            if (threadIdx.x == 0 && a.error) atomicExch(a.error, 3);
+            return false;
+        }
+    } else {
+        tyi = blockIdx.x % tiles_y;
+        xa = (blockIdx.x / tiles_y) * a.chunk_x;
+        xb = min(xa + a.chunk_x, a.nx);
+    }
+    return true;
+}
+
+template <int MAT, int S, int V, bool FULLZ>
+__global__ void __launch_bounds__(512)
+    fz_step_kernel(const __grid_constant__ FzMaps maps, const __grid_constant__ FzParams prm) {
+    const fdtd_step_args &a = prm.a;
+    int tyi, xa, xb;
+    if (!fz_block_range(a, prm.L.ty, a.schedule ? a.schedule + 4 * blockIdx.x : nullptr, tyi, xa, xb))
+        return;
+    fz_run<MAT, S, V, FULLZ>(maps, prm, tyi, xa, xb);
+}
+
+// One grid of a batch: its tensor maps and parameters (64-byte aligned for the
+// tensor maps, read by TMA from global memory).
+struct alignas(64) FzInstance {
+    FzMaps maps;
+    FzParams prm;
+};
+
+// Parameter blocks of the grids of live batches, by slot: constant memory,
+// so a block reads its grid's (uniform) parameters through the constant
+// cache; the tensor maps stay in the global instance table, where TMA reads
+// them.
+constexpr int FZ_BATCH_SLOTS = 128;
+__constant__ FzParams g_batch_prm[FZ_BATCH_SLOTS];
+
+// Many grids advanced by one launch: block b runs schedule entry b =
+// (instance, tile, first plane, end plane); instance i uses constant slot
+// base + i and entry i of the instance table.
+template <int MAT, int S, int V, bool FULLZ>
+__global__ void __launch_bounds__(512)
+    fz_batch_kernel(const FzInstance *__restrict__ inst, int base, int count,
+                    const int *__restrict__ sched) {
+    const int *entry = sched + 4 * blockIdx.x;
+    const int i = entry[0];
+    if (i < 0 || i >= count) return;
+    const FzParams &prm = g_batch_prm[base + i];
+    int tyi, xa, xb;
+    if (!fz_block_range(prm.a, prm.L.ty, entry + 1, tyi, xa, xb)) return;
+    fz_run<MAT, S, V, FULLZ>(inst[i].maps, prm, tyi, xa, xb);
+}
+
 static inline size_t up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 static FzLayout fz_layout(int ty, int P, int RZ, int S, int mat, int chunk_x) {
@@ -662,14 +712,14 @@ int fz_occupancy(const fdtd_step_args &a, int *blocks_per_sm) {
     return 0;
 }
 
-int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
+// Tensor maps and parameters of one grid's launch.
+static int fz_build(const fdtd_step_args &a, FzMaps &maps, FzParams &prm, int &S, int &V,
+                    int &nthreads) {
     int rc = get_encoder();
     if (rc) return rc;
     const int P = a.pitch_z, ty = a.tile_y, RZ = a.psi_rz;
     FzLayout L;
-    int S, V, nthreads;
     if ((rc = fz_shape(a, L, S, V, nthreads))) return rc;
-    FzMaps maps;
     const cuuint64_t nz = a.nz, ny = a.ny, nx = a.nx, pz = P;
     cuuint64_t fdims[4] = {nz, ny, nx, 3};
     cuuint64_t fstr[3] = {pz * 4, pz * ny * 4, pz * ny * nx * 4};
@@ -681,21 +731,18 @@ int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
         if ((rc = encode(&maps.E[j], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, a.E[j], fdims, fstr, ebox)))
             return rc;
     }
+    cuuint64_t mdims[3] = {nz, ny, nx};
+    cuuint32_t mbox[3] = {(cuuint32_t)L.MB, (cuuint32_t)(ty + 1), 1};
     if (a.material_kind == 1) {
         const cuuint64_t mp = a.material_pitch;
-        cuuint64_t mdims[3] = {nz, ny, nx};
         cuuint64_t mstr[2] = {mp, mp * ny};
-        cuuint32_t mbox[3] = {(cuuint32_t)L.MB, (cuuint32_t)(ty + 1), 1};
         if ((rc = encode(&maps.M, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, a.material, mdims, mstr, mbox)))
             return rc;
     } else {
-        cuuint64_t mdims[3] = {nz, ny, nx};
         cuuint64_t mstr[2] = {pz * 4, pz * ny * 4};
-        cuuint32_t mbox[3] = {(cuuint32_t)L.MB, (cuuint32_t)(ty + 1), 1};
         if ((rc = encode(&maps.M, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, a.inv_eps, mdims, mstr, mbox)))
             return rc;
     }
-    FzParams prm;
     prm.a = a;
     prm.L = L;
     prm.xoff = 0;
@@ -718,13 +765,169 @@ int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
     } else {
         maps.PZE[0] = maps.PZE[1] = maps.PZH[0] = maps.PZH[1] = maps.M;  // never loaded
     }
-    const int tiles = (a.ny + ty - 1) / ty;
+    return 0;
+}
+
+int launch_fz(const fdtd_step_args &a, cudaStream_t stream) {
+    FzMaps maps;
+    FzParams prm;
+    int S, V, nthreads, rc;
+    if ((rc = fz_build(a, maps, prm, S, V, nthreads))) return rc;
+    const int tiles = (a.ny + a.tile_y - 1) / a.tile_y;
     const int chunks = (a.nx + a.chunk_x - 1) / a.chunk_x;
     dim3 grid((unsigned)(a.schedule ? a.schedule_blocks : tiles * chunks));
     FzKernel kern = fz_pick(a, S, V);
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.smem_bytes);
-    kern<<<grid, dim3((unsigned)nthreads), L.smem_bytes, stream>>>(maps, prm);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, prm.L.smem_bytes);
+    kern<<<grid, dim3((unsigned)nthreads), prm.L.smem_bytes, stream>>>(maps, prm);
     return launch_status("fdtd_step_fused (full-z TMA)");
 }
 
+// ------------------------------ batches ------------------------------
+
+using FzBatchKernel = void (*)(const FzInstance *, int, int, const int *);
+
+template <int M, int SS>
+static FzBatchKernel fz_pick_batch_v(int V, bool full) {
+    if (full) return V == 4 ? fz_batch_kernel<M, SS, 4, true> : fz_batch_kernel<M, SS, 2, true>;
+    return V == 4 ? fz_batch_kernel<M, SS, 4, false> : fz_batch_kernel<M, SS, 2, false>;
+}
+
+static FzBatchKernel fz_pick_batch(int mat, int S, int V, bool full) {
+    if (mat == 1)
+        return S == 2 ? fz_pick_batch_v<1, 2>(V, full)
+             : S == 3 ? fz_pick_batch_v<1, 3>(V, full) : fz_pick_batch_v<1, 4>(V, full);
+    return S == 2 ? fz_pick_batch_v<0, 2>(V, full)
+         : S == 3 ? fz_pick_batch_v<0, 3>(V, full) : fz_pick_batch_v<0, 4>(V, full);
+}
+
 }  // namespace wfb
+
+using namespace wfb;
+
+// Constant-memory slots of live batches, per device.
+static std::mutex g_slot_mu;
+static bool g_slot_used[64][FZ_BATCH_SLOTS];
+
+static int fz_slots_take(int dev, int count) {
+    std::lock_guard<std::mutex> lock(g_slot_mu);
+    for (int b = 0; b + count <= FZ_BATCH_SLOTS; ++b) {
+        bool free = true;
+        for (int j = b; j < b + count && free; ++j) free = !g_slot_used[dev][j];
+        if (free) {
+            for (int j = b; j < b + count; ++j) g_slot_used[dev][j] = true;
+            return b;
+        }
+    }
+    return -1;
+}
+
+static void fz_slots_give(int dev, int base, int count) {
+    std::lock_guard<std::mutex> lock(g_slot_mu);
+    for (int j = base; j >= 0 && j < base + count && j < FZ_BATCH_SLOTS; ++j) g_slot_used[dev][j] = false;
+}
+
+extern "C" long long fdtd_batch_workspace_bytes(int count) {
+    return count > 0 ? (long long)count * (long long)sizeof(FzInstance) : 0;
+}
+
+extern "C" int fdtd_batch_prepare(const fdtd_step_args *args, int count, void *workspace,
+                                  long long workspace_bytes, fdtd_batch_plan *plan) {
+    if (!args || count < 1 || !workspace || !plan ||
+        workspace_bytes < fdtd_batch_workspace_bytes(count) || ((uintptr_t)workspace & 63)) {
+        set_error("fdtd_batch_prepare: invalid arguments (workspace of "
+                  "fdtd_batch_workspace_bytes(count), 64-byte aligned)");
+        return FDTD_ERR_ARG;
+    }
+    FzInstance *host = new (std::nothrow) FzInstance[count];
+    if (!host) {
+        set_error("fdtd_batch_prepare: host allocation failed");
+        return FDTD_ERR_CUDA;
+    }
+    int rc = 0, S0 = 0, V0 = 0, threads0 = 0;
+    bool full0 = true;
+    for (int i = 0; i < count && !rc; ++i) {
+        fdtd_step_args a = args[i];
+        if (a.pitch_z <= 0) a.pitch_z = a.nz;
+        if (a.material_pitch <= 0) a.material_pitch = a.nz;
+        a.schedule = nullptr;  // the batch schedule takes its place
+        a.schedule_blocks = 0;
+        if (a.nx <= 0 || a.ny <= 0 || a.nz <= 0 || !a.step || a.packed != FDTD_PSI_SLAB ||
+            !fz_eligible(a) || a.tile_y < 1 || a.chunk_x < 1) {
+            set_error("fdtd_batch_prepare: instance %d does not select the full-z path with a set "
+                      "tile_y and chunk_x", i);
+            rc = FDTD_ERR_ARG;
+            break;
+        }
+        int S, V, threads;
+        if ((rc = fz_build(a, host[i].maps, host[i].prm, S, V, threads))) break;
+        const bool full = a.nz == a.pitch_z;
+        if (i == 0) {
+            S0 = S, V0 = V, threads0 = threads, full0 = full;
+        } else if (S != S0 || V != V0 || threads != threads0 || full != full0 ||
+                   host[i].prm.L.smem_bytes != host[0].prm.L.smem_bytes ||
+                   a.material_kind != args[0].material_kind) {
+            set_error("fdtd_batch_prepare: instance %d differs from instance 0 in row pitch, "
+                      "z slab width, material kind, tile or stages", i);
+            rc = FDTD_ERR_ARG;
+        }
+    }
+    int dev = 0, base = -1;
+    if (!rc) {
+        cudaError_t err = cudaGetDevice(&dev);
+        if (err == cudaSuccess && (dev < 0 || dev >= 64)) err = cudaErrorInvalidDevice;
+        if (err == cudaSuccess && (base = fz_slots_take(dev, count)) < 0) {
+            set_error("fdtd_batch_prepare: %d grids exceed the %d free parameter slots of live "
+                      "batches (fdtd_batch_release frees them)", count, FZ_BATCH_SLOTS);
+            rc = FDTD_ERR_ARG;
+        }
+        for (int i = 0; !rc && err == cudaSuccess && i < count; ++i)
+            err = cudaMemcpyToSymbol(g_batch_prm, &host[i].prm, sizeof(FzParams),
+                                     (size_t)(base + i) * sizeof(FzParams));
+        if (!rc && err == cudaSuccess)
+            err = cudaMemcpy(workspace, host, sizeof(FzInstance) * (size_t)count,
+                             cudaMemcpyHostToDevice);
+        if (!rc && err != cudaSuccess) {
+            set_error("fdtd_batch_prepare: %s", cudaGetErrorString(err));
+            rc = FDTD_ERR_CUDA;
+        }
+        if (rc && base >= 0) fz_slots_give(dev, base, count);
+    }
+    if (!rc) {
+        plan->count = count;
+        plan->base = base;
+        plan->device = dev;
+        plan->smem_bytes = host[0].prm.L.smem_bytes;
+        plan->threads = threads0;
+        plan->material_kind = args[0].material_kind;
+        plan->stages = S0;
+        plan->vector = V0;
+        plan->full_rows = full0 ? 1 : 0;
+    }
+    delete[] host;
+    return rc;
+}
+
+extern "C" int fdtd_step_batch(const fdtd_batch_plan *plan, const void *workspace,
+                               const int *schedule, int blocks, void *stream) {
+    if (!plan || !workspace || !schedule || blocks < 1 || plan->count < 1 || plan->base < 0) {
+        set_error("fdtd_step_batch: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    FzBatchKernel kern = fz_pick_batch(plan->material_kind, plan->stages, plan->vector,
+                                       plan->full_rows != 0);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, plan->smem_bytes);
+    kern<<<(unsigned)blocks, (unsigned)plan->threads, plan->smem_bytes, (cudaStream_t)stream>>>(
+        (const FzInstance *)workspace, plan->base, plan->count, schedule);
+    return launch_status("fdtd_step_batch");
+}
+
+extern "C" int fdtd_batch_release(fdtd_batch_plan *plan) {
+    if (!plan || plan->count < 1 || plan->base < 0 || plan->device < 0 || plan->device >= 64) {
+        set_error("fdtd_batch_release: not a prepared plan");
+        return FDTD_ERR_ARG;
+    }
+    fz_slots_give(plan->device, plan->base, plan->count);
+    plan->count = 0;
+    plan->base = -1;
+    return 0;
+}

@@ -14,6 +14,10 @@ so that every resident block slot of the GPU gets one run: one wave, no tail.
 
 import numpy as np
 
+# Longest plane run of a block in a batch (the run length sizes the block's
+# shared-memory x-coefficient table).
+MAX_RUN = 96
+
 # Extra cost of a plane whose tile holds y-slab rows / whose x position is an
 # x-slab plane, relative to an interior plane (B200, 20 nm bend: the best of
 # sweeps over 0.6..1.5 / 0.5..1.3 at tile_y 5 and 6).
@@ -54,4 +58,31 @@ def balanced_schedule(shape, tile_y, coeff_e, coeff_h, blocks, wy=Y_WEIGHT, wx=X
         for a, b in zip(cuts[:-1], cuts[1:]):
             if b > a:
                 entries.append((t, a, b, 0))
+    return np.asarray(entries, np.int32).reshape(-1, 4)
+
+
+def batch_schedule(grids, tile_y, blocks, wy=Y_WEIGHT, wx=X_WEIGHT, max_run=MAX_RUN):
+    """Many grids in one launch: `grids` is a list of (shape, coeff_e,
+    coeff_h); every (grid, tile) gets runs of equal estimated cost, at least
+    `blocks` runs in all (one wave) and runs of about `max_run` planes at
+    most (more waves when the tiles outnumber the slots).  Returns the (n, 4) int32
+    table (grid, y tile, first plane, end plane) of fdtd_step_batch."""
+    costs = [plane_costs(shape, tile_y, ce, ch, wy, wx) for shape, ce, ch in grids]
+    per_tile = np.concatenate([c.sum(axis=1) for c in costs])
+    nx_tile = np.concatenate([np.full(c.shape[0], shape[0]) for c, (shape, _, _) in zip(costs, grids)])
+    least = -(-nx_tile // max_run)  # runs of at most max_run planes
+    total = max(int(blocks), int(least.sum()))
+    share = per_tile / per_tile.sum() * total
+    runs = np.maximum(least, np.floor(share).astype(np.int64))
+    while runs.sum() < total:
+        runs[np.argmax(share - runs)] += 1
+    entries, j = [], 0
+    for g, (c, (shape, _, _)) in enumerate(zip(costs, grids)):
+        nx = shape[0]
+        for t in range(c.shape[0]):
+            n = int(min(runs[j], nx))
+            j += 1
+            cum = np.concatenate([[0.0], np.cumsum(c[t])])
+            cuts = [0] + [int(np.searchsorted(cum, cum[-1] * k / n)) for k in range(1, n)] + [nx]
+            entries += [(g, t, a, b) for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
     return np.asarray(entries, np.int32).reshape(-1, 4)
