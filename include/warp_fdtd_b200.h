@@ -334,6 +334,19 @@ int fdtd_record_stage(const float *E0, const float *E1, const float *H0, const f
                       int nx, int ny, int nz, int pitch_z, int x0, int y0, int z0, int sx,
                       int sy, int sz, int exact, void *stream);
 
+/* fdtd_record_stage for up to FDTD_STAGE_PLANES_MAX planes in one launch
+ * (each plane with its own schedule, staging buffer and extent).  No
+ * reference counterpart. */
+#define FDTD_STAGE_PLANES_MAX 8
+typedef struct fdtd_stage_plane {
+    const int *indices;  /* (nsteps) */
+    float *stage;        /* (T, 6, sx*sy*sz) */
+    int nsteps, T, x0, y0, z0, sx, sy, sz, exact;
+} fdtd_stage_plane;
+int fdtd_record_stage_many(const float *E0, const float *E1, const float *H0, const float *H1,
+                           const int *step, const fdtd_stage_plane *planes, int nplanes, int nx,
+                           int ny, int nz, int pitch_z, void *stream);
+
 /* Fold the steps staged since the last fold into the phasors, in time order:
  * run after fdtd_advance once every T steps and after the last step.  With
  * s = step[0] (steps completed) the window is [T * floor((s - 1) / T), s).

@@ -68,6 +68,13 @@ class StepArgs(ctypes.Structure):
     ]
 
 
+class StagePlane(ctypes.Structure):
+    """Mirror of `fdtd_stage_plane`."""
+
+    _fields_ = [("indices", _p), ("stage", _p)] + [
+        (name, _i) for name in ("nsteps", "T", "x0", "y0", "z0", "sx", "sy", "sz", "exact")]
+
+
 class BatchPlan(ctypes.Structure):
     """Mirror of `fdtd_batch_plan`."""
 
@@ -86,6 +93,8 @@ _SIGNATURES = {
     "fdtd_step_batch": [ctypes.POINTER(BatchPlan), _p, _p, _i, _p],
     "fdtd_advance_many": [_p, _i, _i, _p],
     "fdtd_batch_release": [ctypes.POINTER(BatchPlan)],
+    "fdtd_record_stage_many": [_p, _p, _p, _p, _p, ctypes.POINTER(StagePlane), _i, _i, _i, _i,
+                               _i, _p],
     "fdtd_record_volume": [_p, _p, _p, _p, _p, _p, _ll, _p, _i, _i, _p, _i, _i, _i, _i, _p],
     "fdtd_record": [_p, _p, _p, _ll, _p, _p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i,
                     _i, _i, _i, _i, _p],

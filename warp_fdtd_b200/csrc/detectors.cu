@@ -184,6 +184,39 @@ __global__ void record_volume_kernel(const float *__restrict__ E0, const float *
     }
 }
 
+// fdtd_record_stage over several planes in one launch (blockIdx.y = plane).
+struct StagePlanes {
+    fdtd_stage_plane p[FDTD_STAGE_PLANES_MAX];
+};
+
+__global__ void record_stage_many_kernel(const float *__restrict__ E0, const float *__restrict__ E1,
+                                         const float *__restrict__ H0, const float *__restrict__ H1,
+                                         const int *__restrict__ step, const StagePlanes planes,
+                                         int nx, int ny, int nz, int pitch) {
+    const fdtd_stage_plane &pl = planes.p[blockIdx.y];
+    const i64 count = (i64)pl.sx * pl.sy * pl.sz;
+    const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int t = step[0];
+    if (t < 0 || t >= pl.nsteps || pl.indices[t] < 0) return;
+    const int s = t & 1;
+    const float *e = s ? E0 : E1;
+    const float *h = s ? H0 : H1;
+    const float *prev = s ? H1 : H0;
+    const i64 n = (i64)nx * ny * pitch;
+    const int x = pl.x0 + (int)(i / ((i64)pl.sy * pl.sz));
+    const int y = pl.y0 + (int)((i / pl.sz) % pl.sy);
+    const int z = pl.z0 + (int)(i % pl.sz);
+    float ee[3], hh[3];
+    plane_sample(e, h, prev, n, x, y, z, nx, ny, nz, pl.exact, ee, hh, pitch);
+    float *dst = pl.stage + (i64)(t % pl.T) * 6 * count + i;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        dst[(i64)c * count] = ee[c];
+        dst[(i64)(c + 3) * count] = hh[c];
+    }
+}
+
 // One thread per (component, cell); the window's weights are staged in
 // shared memory ([k][t] float2).
 __global__ void dft_fold_kernel(const int *__restrict__ step, const int *__restrict__ indices,
@@ -210,19 +243,32 @@ __global__ void dft_fold_kernel(const int *__restrict__ step, const int *__restr
     if (gid >= 6 * count) return;
     const int c = (int)(gid / count);
     const i64 i = gid - (i64)c * count;
-    for (int k = 0; k < nfreq; ++k) {
-        double2 *p = phasor + ((i64)k * 6 + c) * count + i;
-        double2 acc = *p;
-        for (int dt = 0; dt < n; ++dt) {
-            if (!valid[dt]) continue;
-            const float2 w = wsm[k * T + dt];
-            const double wr = w.x, wi = w.y;
-            if (wr == 0.0 && wi == 0.0) continue;
-            const double v = (double)stage[((i64)((t0 + dt) % T) * 6 + c) * count + i];
-            acc.x = acc.x + wr * v;
-            acc.y = acc.y + wi * v;
+    // the staged samples, 32 steps at a time, read once into registers for all
+    // frequencies; each phasor still sums its steps in time order
+    constexpr int CH = 32;
+    for (int d0 = 0; d0 < n; d0 += CH) {
+        float v[CH];
+#pragma unroll
+        for (int j = 0; j < CH; ++j) {
+            const int dt = d0 + j;
+            v[j] = dt < n && valid[dt] ? stage[((i64)((t0 + dt) % T) * 6 + c) * count + i] : 0.0f;
         }
-        *p = acc;
+        for (int k = 0; k < nfreq; ++k) {
+            double2 *p = phasor + ((i64)k * 6 + c) * count + i;
+            double2 acc = *p;
+#pragma unroll
+            for (int j = 0; j < CH; ++j) {
+                const int dt = d0 + j;
+                if (dt >= n || !valid[dt]) continue;
+                const float2 w = wsm[k * T + dt];
+                const double wr = w.x, wi = w.y;
+                if (wr == 0.0 && wi == 0.0) continue;
+                const double vv = (double)v[j];
+                acc.x = acc.x + wr * vv;
+                acc.y = acc.y + wi * vv;
+            }
+            *p = acc;
+        }
     }
 }
 
@@ -320,6 +366,34 @@ int fdtd_record_volume(const float *E0, const float *E1, const float *H0, const 
         E0, E1, H0, H1, step, positions, (i64)count, (const float2 *)weights, nsteps, first,
         (double2 *)phasor, nx, ny, nz, pitch_z);
     return launch_status("fdtd_record_volume");
+}
+
+int fdtd_record_stage_many(const float *E0, const float *E1, const float *H0, const float *H1,
+                           const int *step, const fdtd_stage_plane *planes, int nplanes, int nx,
+                           int ny, int nz, int pitch_z, void *stream) {
+    if (pitch_z <= 0) pitch_z = nz;
+    if (!planes || nplanes < 1 || nplanes > FDTD_STAGE_PLANES_MAX || !E0 || !E1 || !H0 || !H1 ||
+        !step || pitch_z < nz) {
+        set_error("fdtd_record_stage_many: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    StagePlanes sp;
+    i64 most = 0;
+    for (int j = 0; j < nplanes; ++j) {
+        const fdtd_stage_plane &pl = planes[j];
+        const i64 count = (i64)pl.sx * pl.sy * pl.sz;
+        if (count <= 0 || pl.T < 1 || pl.T > 256 || pl.nsteps < 1 || !pl.indices || !pl.stage ||
+            pl.x0 < 0 || pl.y0 < 0 || pl.z0 < 0 || pl.x0 + pl.sx > nx || pl.y0 + pl.sy > ny ||
+            pl.z0 + pl.sz > nz) {
+            set_error("fdtd_record_stage_many: invalid plane %d", j);
+            return FDTD_ERR_ARG;
+        }
+        sp.p[j] = pl;
+        most = count > most ? count : most;
+    }
+    record_stage_many_kernel<<<dim3((unsigned)((most + 255) / 256), (unsigned)nplanes), 256, 0,
+                               (cudaStream_t)stream>>>(E0, E1, H0, H1, step, sp, nx, ny, nz, pitch_z);
+    return launch_status("fdtd_record_stage_many");
 }
 
 }  // extern "C"

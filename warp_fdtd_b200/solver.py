@@ -522,14 +522,42 @@ class Solver:
             raise ValueError("Trajectory complete; call reset() before stepping again")
         stream = _lib.stream_handle(self.device)
         _lib.call("fdtd_step_fused", self._args, stream)
+        planes, grouped = self._staged_planes()
         for monitor in self.monitors:
-            monitor.launch(self)
+            if id(monitor) not in grouped:
+                monitor.launch(self)
+        if grouped:
+            # every staged phasor plane in one launch
+            nx, ny, nz = self.shape
+            _lib.call("fdtd_record_stage_many", ptr(self._E[0]), ptr(self._E[1]),
+                      ptr(self._H[0]), ptr(self._H[1]), ptr(self.step), planes, len(planes),
+                      nx, ny, nz, self._pitch, stream)
         _lib.call("fdtd_advance", ptr(self.step), 1, stream)
         self._issued += 1
         for monitor in self.monitors:
             if monitor.is_phasor and (self._issued % monitor.batch == 0
                                       or self._issued == self.steps):
                 monitor.fold(self, self._issued)
+
+    def _staged_planes(self):
+        """The staged phasor monitors that share one recording launch: two to
+        eight planes (else none, and each monitor records itself)."""
+        mons = [m for m in self.monitors if getattr(m, "is_phasor", False)
+                and m.shared is None and getattr(m, "stage", None) is not None]
+        key = tuple(id(m) for m in mons)
+        if getattr(self, "_staged_key", None) != key:
+            self._staged_key = key
+            self._staged = (None, frozenset())
+            if 2 <= len(mons) <= 8:
+                planes = (_lib.StagePlane * len(mons))()
+                for pl, m in zip(planes, mons):
+                    pl.indices, pl.stage = ptr(m.indices), ptr(m.stage)
+                    pl.nsteps, pl.T = int(m.indices.numel()), int(m.batch)
+                    pl.x0, pl.y0, pl.z0 = (int(v) for v in m.lo)
+                    pl.sx, pl.sy, pl.sz = (int(v) for v in m.shape)
+                    pl.exact = int(m.exact)
+                self._staged = (planes, frozenset(key))
+        return self._staged
 
     def compile(self):
         start = time.perf_counter()
