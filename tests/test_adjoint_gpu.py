@@ -59,3 +59,39 @@ def test_checkpoint_interval_does_not_change_the_gradient(grad20):
     assert loss2 == loss
     assert rel(full.grad.cpu().numpy(), adj.grad.cpu().numpy()) < 1e-5
     assert rel(grad2, grad) < 1e-5
+
+
+def test_gradient_matches_central_differences(grad20):
+    """The whole chain (parameters -> material map -> FDTD -> modal T) against
+    central finite differences, h = 1e-3, on 16 seeded pixels drawn from the
+    upper quartile of |gradient| (smaller entries move T by less than the
+    float32 trajectory resolves; even in the quartile a few pixels change T by
+    only ~1e-6, so the bar is on the aggregate and the median)."""
+    from warp_fdtd_b200.detectors import measurements
+
+    adj, p0, loss, grad = grad20
+    g = np.asarray(grad, np.float64).ravel()
+    rng = np.random.default_rng(16)
+    top = np.flatnonzero(np.abs(g) >= np.quantile(np.abs(g), 0.75))
+    pixels = rng.choice(top, 16, replace=False)
+    h = 1e-3
+
+    def transmission(p):
+        adj.set_design(p.reshape(p0.shape))
+        adj.reset()
+        adj.run()
+        return measurements(adj)["modal_transmission"]
+
+    fd = []
+    for j in pixels:
+        pp, pm = p0.ravel().copy(), p0.ravel().copy()
+        pp[j] += h
+        pm[j] -= h
+        fd.append(-(transmission(pp) - transmission(pm)) / (2 * h))
+    fd = np.array(fd)
+    err = np.abs(fd - g[pixels]) / np.abs(g[pixels])
+    print("FD vs adjoint per-pixel relative errors:", np.round(err, 4), "rel-L2", rel(fd, g[pixels]))
+    # measured on a B200: rel-L2 1.05e-2, median per-pixel error 6e-3, the two
+    # smallest pixels at 0.12 and 0.18 (T moves by ~1e-6 there)
+    assert rel(fd, g[pixels]) < 0.02
+    assert np.median(err) < 0.01
