@@ -272,7 +272,7 @@ def run_ours(args, world, rank, local):
     # monitor's folds (every `batch` steps and at the end)
     planes, grouped = s._staged_planes()
     own = sum(1 for m in s.monitors if m.shared is None and id(m) not in grouped)
-    launches_per_step = 1 + own + (1 if grouped else 0) + 1
+    launches_per_step = 1 + own + 1  # the grouped recorder also advances the counter
     folds = sum(-(-s.steps // m.batch) for m in s.monitors if m.is_phasor and m.shared is None)
 
     # dominant kernel alone: average duration of the fused step over 200 launches

@@ -335,8 +335,11 @@ int fdtd_record_stage(const float *E0, const float *E1, const float *H0, const f
                       int sy, int sz, int exact, void *stream);
 
 /* fdtd_record_stage for up to FDTD_STAGE_PLANES_MAX planes in one launch
- * (each plane with its own schedule, staging buffer and extent).  No
- * reference counterpart. */
+ * (each plane with its own schedule, staging buffer and extent).  With
+ * advance_counter (a device unsigned, zero before the first call) the launch
+ * also advances step[0] by delta once every block has read it, in place of a
+ * following fdtd_advance; the counter is left at zero.  No reference
+ * counterpart. */
 #define FDTD_STAGE_PLANES_MAX 8
 typedef struct fdtd_stage_plane {
     const int *indices;  /* (nsteps) */
@@ -344,8 +347,9 @@ typedef struct fdtd_stage_plane {
     int nsteps, T, x0, y0, z0, sx, sy, sz, exact;
 } fdtd_stage_plane;
 int fdtd_record_stage_many(const float *E0, const float *E1, const float *H0, const float *H1,
-                           const int *step, const fdtd_stage_plane *planes, int nplanes, int nx,
-                           int ny, int nz, int pitch_z, void *stream);
+                           int *step, const fdtd_stage_plane *planes, int nplanes, int nx,
+                           int ny, int nz, int pitch_z, unsigned *advance_counter, int delta,
+                           void *stream);
 
 /* Fold the steps staged since the last fold into the phasors, in time order:
  * run after fdtd_advance once every T steps and after the last step.  With

@@ -189,32 +189,49 @@ struct StagePlanes {
     fdtd_stage_plane p[FDTD_STAGE_PLANES_MAX];
 };
 
+// With `done` set, the block that finishes last also advances step[0] by
+// `delta` (every block has read it by then) and rearms the counter.
+__device__ __forceinline__ void stage_block_done(int *step, unsigned *done, int delta) {
+    if (!done) return;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned blocks = gridDim.x * gridDim.y;
+        if (atomicAdd(done, 1u) == blocks - 1) {
+            step[0] += delta;
+            *done = 0;
+            __threadfence();
+        }
+    }
+}
+
 __global__ void record_stage_many_kernel(const float *__restrict__ E0, const float *__restrict__ E1,
                                          const float *__restrict__ H0, const float *__restrict__ H1,
-                                         const int *__restrict__ step, const StagePlanes planes,
-                                         int nx, int ny, int nz, int pitch) {
+                                         int *step, const StagePlanes planes, int nx, int ny,
+                                         int nz, int pitch, unsigned *done, int delta) {
     const fdtd_stage_plane &pl = planes.p[blockIdx.y];
     const i64 count = (i64)pl.sx * pl.sy * pl.sz;
     const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
-    const int t = step[0];
-    if (t < 0 || t >= pl.nsteps || pl.indices[t] < 0) return;
-    const int s = t & 1;
-    const float *e = s ? E0 : E1;
-    const float *h = s ? H0 : H1;
-    const float *prev = s ? H1 : H0;
-    const i64 n = (i64)nx * ny * pitch;
-    const int x = pl.x0 + (int)(i / ((i64)pl.sy * pl.sz));
-    const int y = pl.y0 + (int)((i / pl.sz) % pl.sy);
-    const int z = pl.z0 + (int)(i % pl.sz);
-    float ee[3], hh[3];
-    plane_sample(e, h, prev, n, x, y, z, nx, ny, nz, pl.exact, ee, hh, pitch);
-    float *dst = pl.stage + (i64)(t % pl.T) * 6 * count + i;
+    const int t = *(volatile int *)step;
+    if (i < count && t >= 0 && t < pl.nsteps && pl.indices[t] >= 0) {
+        const int s = t & 1;
+        const float *e = s ? E0 : E1;
+        const float *h = s ? H0 : H1;
+        const float *prev = s ? H1 : H0;
+        const i64 n = (i64)nx * ny * pitch;
+        const int x = pl.x0 + (int)(i / ((i64)pl.sy * pl.sz));
+        const int y = pl.y0 + (int)((i / pl.sz) % pl.sy);
+        const int z = pl.z0 + (int)(i % pl.sz);
+        float ee[3], hh[3];
+        plane_sample(e, h, prev, n, x, y, z, nx, ny, nz, pl.exact, ee, hh, pitch);
+        float *dst = pl.stage + (i64)(t % pl.T) * 6 * count + i;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        dst[(i64)c * count] = ee[c];
-        dst[(i64)(c + 3) * count] = hh[c];
+        for (int c = 0; c < 3; ++c) {
+            dst[(i64)c * count] = ee[c];
+            dst[(i64)(c + 3) * count] = hh[c];
+        }
     }
+    stage_block_done(step, done, delta);  // every thread of the block reaches it
 }
 
 // One thread per (component, cell); the window's weights are staged in
@@ -369,8 +386,9 @@ int fdtd_record_volume(const float *E0, const float *E1, const float *H0, const 
 }
 
 int fdtd_record_stage_many(const float *E0, const float *E1, const float *H0, const float *H1,
-                           const int *step, const fdtd_stage_plane *planes, int nplanes, int nx,
-                           int ny, int nz, int pitch_z, void *stream) {
+                           int *step, const fdtd_stage_plane *planes, int nplanes, int nx,
+                           int ny, int nz, int pitch_z, unsigned *advance_counter, int delta,
+                           void *stream) {
     if (pitch_z <= 0) pitch_z = nz;
     if (!planes || nplanes < 1 || nplanes > FDTD_STAGE_PLANES_MAX || !E0 || !E1 || !H0 || !H1 ||
         !step || pitch_z < nz) {
@@ -392,7 +410,8 @@ int fdtd_record_stage_many(const float *E0, const float *E1, const float *H0, co
         most = count > most ? count : most;
     }
     record_stage_many_kernel<<<dim3((unsigned)((most + 255) / 256), (unsigned)nplanes), 256, 0,
-                               (cudaStream_t)stream>>>(E0, E1, H0, H1, step, sp, nx, ny, nz, pitch_z);
+                               (cudaStream_t)stream>>>(E0, E1, H0, H1, step, sp, nx, ny, nz, pitch_z,
+                                                       advance_counter, delta);
     return launch_status("fdtd_record_stage_many");
 }
 

@@ -211,6 +211,7 @@ class Solver:
         self._H = [torch.zeros((3, self._cells), **f32) for _ in range(2)]
         self._issued = 0
         self.step = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._advance_counter = torch.zeros(1, dtype=torch.int32, device=dev)
 
         # materials: uint8 index + table when possible, else float32 per cell
         flat = np.ascontiguousarray(eps.reshape(-1), np.float32)
@@ -527,12 +528,14 @@ class Solver:
             if id(monitor) not in grouped:
                 monitor.launch(self)
         if grouped:
-            # every staged phasor plane in one launch
+            # every staged phasor plane in one launch, which also advances the
+            # step counter after all of its blocks have read it
             nx, ny, nz = self.shape
             _lib.call("fdtd_record_stage_many", ptr(self._E[0]), ptr(self._E[1]),
                       ptr(self._H[0]), ptr(self._H[1]), ptr(self.step), planes, len(planes),
-                      nx, ny, nz, self._pitch, stream)
-        _lib.call("fdtd_advance", ptr(self.step), 1, stream)
+                      nx, ny, nz, self._pitch, ptr(self._advance_counter), 1, stream)
+        else:
+            _lib.call("fdtd_advance", ptr(self.step), 1, stream)
         self._issued += 1
         for monitor in self.monitors:
             if monitor.is_phasor and (self._issued % monitor.batch == 0
