@@ -256,13 +256,18 @@ __global__ void dft_fold_kernel(const int *__restrict__ step, const int *__restr
         valid[j] = (j < n && t < nsteps && indices[t] >= 0) ? 1 : 0;
     }
     __syncthreads();
+    // one thread per (frequency, component, cell): the staged samples of a
+    // cell are read (from L2) by its frequencies' threads; each phasor sums its
+    // steps in time order
     const i64 gid = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= 6 * count) return;
-    const int c = (int)(gid / count);
-    const i64 i = gid - (i64)c * count;
-    // the staged samples, 32 steps at a time, read once into registers for all
-    // frequencies; each phasor still sums its steps in time order
-    constexpr int CH = 32;
+    if (gid >= (i64)nfreq * 6 * count) return;
+    const int k = (int)(gid / (6 * count));
+    const i64 rem = gid - (i64)k * 6 * count;
+    const int c = (int)(rem / count);
+    const i64 i = rem - (i64)c * count;
+    double2 *p = phasor + ((i64)k * 6 + c) * count + i;
+    double2 acc = *p;
+    constexpr int CH = 8;  // samples in flight per thread
     for (int d0 = 0; d0 < n; d0 += CH) {
         float v[CH];
 #pragma unroll
@@ -270,23 +275,19 @@ __global__ void dft_fold_kernel(const int *__restrict__ step, const int *__restr
             const int dt = d0 + j;
             v[j] = dt < n && valid[dt] ? stage[((i64)((t0 + dt) % T) * 6 + c) * count + i] : 0.0f;
         }
-        for (int k = 0; k < nfreq; ++k) {
-            double2 *p = phasor + ((i64)k * 6 + c) * count + i;
-            double2 acc = *p;
 #pragma unroll
-            for (int j = 0; j < CH; ++j) {
-                const int dt = d0 + j;
-                if (dt >= n || !valid[dt]) continue;
-                const float2 w = wsm[k * T + dt];
-                const double wr = w.x, wi = w.y;
-                if (wr == 0.0 && wi == 0.0) continue;
-                const double vv = (double)v[j];
-                acc.x = acc.x + wr * vv;
-                acc.y = acc.y + wi * vv;
-            }
-            *p = acc;
+        for (int j = 0; j < CH; ++j) {
+            const int dt = d0 + j;
+            if (dt >= n || !valid[dt]) continue;
+            const float2 w = wsm[k * T + dt];
+            const double wr = w.x, wi = w.y;
+            if (wr == 0.0 && wi == 0.0) continue;
+            const double vv = (double)v[j];
+            acc.x = acc.x + wr * vv;
+            acc.y = acc.y + wi * vv;
         }
     }
+    *p = acc;
 }
 
 }  // namespace wfb
@@ -361,7 +362,7 @@ int fdtd_dft_fold(const int *step, const int *indices, int nsteps, const float *
         set_error("fdtd_dft_fold: invalid arguments");
         return FDTD_ERR_ARG;
     }
-    const i64 work = 6 * (i64)count;
+    const i64 work = (i64)nfreq * 6 * count;
     const size_t smem = (size_t)nfreq * T * sizeof(float2);
     dft_fold_kernel<<<(unsigned)((work + 255) / 256), 256, smem, (cudaStream_t)stream>>>(
         step, indices, nsteps, (const float2 *)weights, nfreq, stage, T, (double2 *)phasor,
