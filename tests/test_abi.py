@@ -16,7 +16,8 @@ def declared_symbols():
     for header in (ROOT / "include").glob("*.h"):
         text = header.read_text()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        names.update(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(fdtd_\w+)\s*\(", text, flags=re.M))
+        names.update(re.findall(r"^\s*(?:const\s+)?(?:\w+\s+)*\w+\s*\*?\s*(fdtd_\w+)\s*\(", text,
+                                flags=re.M))
     return sorted(names)
 
 
@@ -58,3 +59,27 @@ def test_argument_errors_need_no_gpu(lib):
     rc = lib.fdtd_advance(None, 1, None)
     assert rc == -1
     assert b"null" in lib.fdtd_last_error()
+
+
+def test_new_entry_points_reject_bad_arguments(lib):
+    """Batches, grouped staging, the volume recorder and the launch-shape
+    queries check their arguments on the host."""
+    from warp_fdtd_b200 import _lib
+
+    L = _lib.load()
+    assert L.fdtd_batch_workspace_bytes(0) == 0
+    assert L.fdtd_batch_workspace_bytes(3) > 0
+    plan = _lib.BatchPlan()
+    assert L.fdtd_batch_prepare(None, 0, None, 0, ctypes.byref(plan)) == -1
+    assert L.fdtd_step_batch(ctypes.byref(plan), None, None, 0, None) == -1
+    assert L.fdtd_batch_release(ctypes.byref(plan)) == -1
+    assert L.fdtd_advance_many(None, 0, 1, None) == -1
+    assert L.fdtd_record_stage_many(None, None, None, None, None, None, 0, 8, 8, 8, 8, None, 0,
+                                    None) == -1
+    assert L.fdtd_record_volume(None, None, None, None, None, None, 0, None, 1, 0, None, 4, 4, 4,
+                                4, None) == -1
+    a = _lib.StepArgs()
+    assert L.fdtd_step_defaults(ctypes.byref(a)) == -1
+    blocks, sms = ctypes.c_int(), ctypes.c_int()
+    assert L.fdtd_step_occupancy(ctypes.byref(a), ctypes.byref(blocks), ctypes.byref(sms)) == -1
+    assert b"full-z" in L.fdtd_last_error()

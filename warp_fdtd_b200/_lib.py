@@ -121,7 +121,8 @@ _SIGNATURES = {
                            _i, _i, _i, _i, _i, _p],
 }
 
-EXPORTS = sorted(_SIGNATURES) + ["fdtd_last_error", "fdtd_version"]
+EXPORTS = sorted(_SIGNATURES) + ["fdtd_batch_workspace_bytes", "fdtd_last_error",
+                                 "fdtd_version"]
 
 _lib = None
 
