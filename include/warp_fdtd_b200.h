@@ -362,6 +362,109 @@ int fdtd_dft_fold(const int *step, const int *indices, int nsteps, const float *
                   int nfreq, const float *stage, int T, double *phasor, long long count,
                   void *stream);
 
+/* ---------------------------------------------------------------------------
+ * 4. CNN surrogate (no reference counterpart: the reference optimises with
+ *    the adjoint alone).  A 2-D encoder-decoder maps a design density to the
+ *    modal transmission at several wavelengths and to the transmission
+ *    gradient map; the design loop uses it to propose updates that a full
+ *    FDTD forward accepts or rejects.  bf16 storage, float32 accumulation.
+ *    Activations are NHWC (pixel p = (b*H + y)*W + x, channel fastest) with a
+ *    row stride ld in elements; im2col column k = tap*C + c, tap = (dy+1)*3 +
+ *    (dx+1).  bf16 buffers are passed as void pointers.
+ * ------------------------------------------------------------------------ */
+
+/* C[M, N] = A[M, K] . B[N, K]^T on the tcgen05 tensor cores (128 x BN tiles,
+ * BN = 32, 64 or 128 picked from N, TMA-staged operands, float32 accumulator
+ * in tensor memory).  A and B are bf16, K contiguous, 16-byte aligned, row
+ * strides lda, ldb multiples of 8; rows and K columns past M, N, K read as
+ * zero.  C is float32 (c_bf16 = 0) or bf16 (c_bf16 = 1, round to nearest
+ * even) with row stride ldc; epilogue: + bias[n] (if bias), + C (accumulate,
+ * float32 only), max(., 0) (relu).  splits > 1 divides K over that many
+ * blocks (fewer when K has fewer 64-wide chunks; fdtd_sg_gemm_splits gives
+ * the count used), each writing its float32 partial at C + z*split_stride,
+ * with no bias, relu or accumulate: sum them with fdtd_sg_splitk_reduce.
+ * layout picks the shared-memory operand layout: 0 = 128-byte swizzled rows
+ * (one TMA box per operand and stage), 1 = interleaved 8 x 16-byte core
+ * matrices (eight narrow boxes); results are identical. */
+typedef struct fdtd_sg_gemm_args {
+    const void *A;
+    int lda;
+    const void *B;
+    int ldb;
+    void *C;
+    int ldc;
+    int c_bf16;
+    const float *bias;
+    int M, N, K;
+    int splits;
+    long long split_stride;
+    int accumulate;
+    int relu;
+    int layout;
+} fdtd_sg_gemm_args;
+int fdtd_sg_gemm(const fdtd_sg_gemm_args *args, void *stream);
+/* Number of K splits fdtd_sg_gemm uses for these arguments. */
+int fdtd_sg_gemm_splits(const fdtd_sg_gemm_args *args);
+/* Copies the GEMM wait status to *out (0: every bounded mbarrier wait
+ * completed; 1: one ran out and its tile was not written); reset != 0 clears
+ * it.  Synchronous. */
+int fdtd_sg_status(int *out, int reset);
+
+/* col[p, tap*C + c] = x[p + offset(tap), c] with zero padding (3 x 3, same
+ * size); columns past 9*C are left untouched. */
+int fdtd_sg_im2col(const void *x, int ldx, int B, int H, int W, int C, void *col, int ldcol,
+                   void *stream);
+/* dst[c, r] = src[r, c] (bf16). */
+int fdtd_sg_transpose(const void *src, int lds, long long rows, int cols, void *dst,
+                      long long ldd, void *stream);
+/* Adjoint of im2col: dx[p, c] (+)= sum over taps of dcol[p - offset(tap), tap*C + c]. */
+int fdtd_sg_col2im(const float *dcol, int ldd, int B, int H, int W, int C, float *dx, int ldx,
+                   int accumulate, void *stream);
+/* dz = bf16(y > 0 ? dy : 0) and bias_grad[c] = sum_p of the same masked values
+ * (scratch: 64*C floats). */
+int fdtd_sg_relu_backward(const float *dy, int lddy, const void *y, int ldy, long long P, int C,
+                          void *dz, int ldz, float *bias_grad, float *scratch, void *stream);
+/* 2 x 2 average pool of an H x W map (H, W even) and its adjoint. */
+int fdtd_sg_pool(const void *x, int ldx, int B, int H, int W, int C, void *y, int ldy,
+                 void *stream);
+int fdtd_sg_pool_backward(const float *dy, int lddy, int B, int H, int W, int C, float *dx,
+                          int ldx, int accumulate, void *stream);
+/* Nearest 2x upsample of an H x W map and its adjoint (H, W: the small map). */
+int fdtd_sg_upsample(const void *x, int ldx, int B, int H, int W, int C, void *y, int ldy,
+                     void *stream);
+int fdtd_sg_upsample_backward(const float *dy, int lddy, int B, int H, int W, int C, float *dx,
+                              int ldx, int accumulate, void *stream);
+/* Transmission head: feat[b, c] = mean_p x[b, p, c]; out[b, k] = bl[k] +
+ * sum_c feat[b, c] * Wl[k, c] (float32 Wl [K, C]); and its reverse mode. */
+int fdtd_sg_gap_linear(const void *x, int ldx, int B, int npix, int C, const float *Wl,
+                       const float *bl, int K, float *feat, float *out, void *stream);
+int fdtd_sg_gap_linear_backward(const float *dout, const float *feat, const float *Wl, int B,
+                                int npix, int C, int K, float *dWl, float *dbl, float *dx,
+                                int ldx, int accumulate, void *stream);
+/* Gradient-map head: out[p] = bg + sum_c x[p, c] * wg[c]; and its reverse
+ * mode (dx overwritten; scratch: 64*C floats). */
+int fdtd_sg_head(const void *x, int ldx, long long P, int C, const float *wg, const float *bg,
+                 float *out, void *stream);
+int fdtd_sg_head_backward(const float *dout, const void *x, int ldx, long long P, int C,
+                          const float *wg, float *dx, int lddx, float *dwg, float *dbg,
+                          float *scratch, void *stream);
+/* grad = scale * 2 * (pred - target); partial[i] = sum of squared
+ * differences of block i (ceil(n / 256) blocks). */
+int fdtd_sg_mse(const float *pred, const float *target, long long n, float scale, float *grad,
+                float *partial, void *stream);
+/* One Adam step (step >= 1: bias corrections 1 - b^step). */
+int fdtd_sg_adam(float *w, const float *g, float *m, float *v, long long n, float lr, float b1,
+                 float b2, float eps, int step, void *stream);
+/* bf16 copies of a float32 [cout, kw] weight: wb [cout, ldw], wt [kw, cout]
+ * (wt may be NULL). */
+int fdtd_sg_cast_weights(const float *w, int cout, int kw, void *wb, int ldw, void *wt,
+                         void *stream);
+/* out = sum_z part[z] (z ascending) for [M, N] partials split_stride apart;
+ * transpose != 0 writes out[n, m]. */
+int fdtd_sg_splitk_reduce(const float *part, int splits, long long stride, int M, int N, int ldp,
+                          float *out, int ldo, int transpose, void *stream);
+int fdtd_sg_to_bf16(const float *x, void *y, long long n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

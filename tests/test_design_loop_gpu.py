@@ -1,0 +1,57 @@
+"""The surrogate-proposed design loop on a small 40 nm bend: what the trained
+CNN gains over the adjoint-only method, on data the solver generates here."""
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small(tmp_path_factory):
+    """A 40 nm bend (radius 1 um, 96 x 96 x 46 cells with an 8-cell CPML) with
+    a 32 x 32 design box over the arc, 2000 steps; triples from four short
+    adjoint trajectories for training and one more held out."""
+    from warp_fdtd_b200 import scene
+    from warp_fdtd_b200.design_loop import DesignProblem, generate
+
+    case = scene.bend_case(tmp_path_factory.mktemp("bend40") / "case", spacing_nm=40.0,
+                           interior_um=(3.2, 3.2, 1.2), pml=8, steps=2000, radius_um=1.0,
+                           nwav=1, pulse_width_fs=50.0)
+    problem = DesignProblem(case, box=(23, 43, 20, 32, 32, 6))
+    data = generate(problem, seeds=[1, 2, 3, 4], steps=8, step=0.1)
+    n_train = len(data)
+    generate(problem, seeds=[100], steps=8, step=0.1, data=data)
+    return problem, data, n_train
+
+
+def test_spectrum_and_gradient_shapes(small):
+    problem, data, n_train = small
+    assert len(data) == n_train + 8
+    assert data.p[0].shape == (32, 32) and data.g[0].shape == (32, 32)
+    assert data.T[0].shape == (8,)
+    T = np.array([t for t in data.T])
+    assert np.isfinite(T).all() and (T >= 0).all()
+    assert all(np.isfinite(g).all() and np.abs(g).max() > 0 for g in data.g)
+
+
+def test_trained_surrogate_predicts_held_out_gradients(small):
+    """Held-out gradient maps (a trajectory from a seed the network never saw):
+    the trained network's predictions point along the exact adjoint gradients,
+    an untrained network's do not."""
+    from warp_fdtd_b200.design_loop import held_out_cosine
+    from warp_fdtd_b200.surrogate import Surrogate
+
+    problem, data, n_train = small
+    net = Surrogate(problem.shape, problem.nwav, seed=0)
+    held = list(range(n_train, len(data)))
+    before = held_out_cosine(net, data, held)
+    P, T, G = data.tensors()
+    net.fit(P[:n_train], T[:n_train], G[:n_train], steps=400, batch=16, lr=1e-3)
+    after = held_out_cosine(net, data, held)
+    Tp, _ = net.predict(P[n_train:])
+    rmse = float(torch.sqrt(torch.mean((Tp - T[n_train:]) ** 2)))
+    print(f"held-out gradient cosine {before:.3f} -> {after:.3f}; spectrum RMSE {rmse:.4f}")
+    # measured on a B200: 0.03 -> 0.30 (and 0.03 -> 0.23 on the 20 nm bend)
+    assert after > 0.15 and after > before + 0.15

@@ -82,6 +82,14 @@ class BatchPlan(ctypes.Structure):
                                         "stages", "vector", "full_rows", "base", "device")]
 
 
+class SgGemmArgs(ctypes.Structure):
+    """Mirror of `fdtd_sg_gemm_args`."""
+
+    _fields_ = [("A", _p), ("lda", _i), ("B", _p), ("ldb", _i), ("C", _p), ("ldc", _i),
+                ("c_bf16", _i), ("bias", _p), ("M", _i), ("N", _i), ("K", _i), ("splits", _i),
+                ("split_stride", _ll), ("accumulate", _i), ("relu", _i), ("layout", _i)]
+
+
 # name -> argtypes (all return int status)
 _SIGNATURES = {
     "fdtd_update": [_i, _i, _p, _p, _ll, _p, _p, _ll, _p, _i, _p, _ll, _p, _ll, _p, _p, _ll,
@@ -117,6 +125,26 @@ _SIGNATURES = {
     "fdtd_record_stage": [_p, _p, _p, _p, _p, _p, _i, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i,
                           _i, _i, _i, _p],
     "fdtd_dft_fold": [_p, _p, _i, _p, _i, _p, _i, _p, _ll, _p],
+    "fdtd_sg_gemm": [ctypes.POINTER(SgGemmArgs), _p],
+    "fdtd_sg_gemm_splits": [ctypes.POINTER(SgGemmArgs)],
+    "fdtd_sg_status": [ctypes.POINTER(_i), _i],
+    "fdtd_sg_im2col": [_p, _i, _i, _i, _i, _i, _p, _i, _p],
+    "fdtd_sg_transpose": [_p, _i, _ll, _i, _p, _ll, _p],
+    "fdtd_sg_col2im": [_p, _i, _i, _i, _i, _i, _p, _i, _i, _p],
+    "fdtd_sg_relu_backward": [_p, _i, _p, _i, _ll, _i, _p, _i, _p, _p, _p],
+    "fdtd_sg_pool": [_p, _i, _i, _i, _i, _i, _p, _i, _p],
+    "fdtd_sg_pool_backward": [_p, _i, _i, _i, _i, _i, _p, _i, _i, _p],
+    "fdtd_sg_upsample": [_p, _i, _i, _i, _i, _i, _p, _i, _p],
+    "fdtd_sg_upsample_backward": [_p, _i, _i, _i, _i, _i, _p, _i, _i, _p],
+    "fdtd_sg_gap_linear": [_p, _i, _i, _i, _i, _p, _p, _i, _p, _p, _p],
+    "fdtd_sg_gap_linear_backward": [_p, _p, _p, _i, _i, _i, _i, _p, _p, _p, _i, _i, _p],
+    "fdtd_sg_head": [_p, _i, _ll, _i, _p, _p, _p, _p],
+    "fdtd_sg_head_backward": [_p, _p, _i, _ll, _i, _p, _p, _i, _p, _p, _p, _p],
+    "fdtd_sg_mse": [_p, _p, _ll, _f, _p, _p, _p],
+    "fdtd_sg_adam": [_p, _p, _p, _p, _ll, _f, _f, _f, _f, _i, _p],
+    "fdtd_sg_cast_weights": [_p, _i, _i, _p, _i, _p, _p],
+    "fdtd_sg_splitk_reduce": [_p, _i, _ll, _i, _i, _i, _p, _i, _i, _p],
+    "fdtd_sg_to_bf16": [_p, _p, _ll, _p],
     "fdtd_record_flux64": [_p, _p, _p, _p, _p, _p, _i, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i,
                            _i, _i, _i, _i, _i, _p],
 }

@@ -79,10 +79,11 @@ inline int get_encoder() {
 }
 
 inline int encode(CUtensorMap *map, CUtensorMapDataType dt, int rank, const void *base,
-                  const cuuint64_t *dims, const cuuint64_t *strides, const cuuint32_t *box) {
+                  const cuuint64_t *dims, const cuuint64_t *strides, const cuuint32_t *box,
+                  CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE) {
     cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = g_encode(map, dt, rank, const_cast<void *>(base), dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle,
                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
