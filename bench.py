@@ -231,6 +231,39 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def surrogate_train_rate(steps=20, warmup=3):
+    """The CNN surrogate's training step (32 designs of 80 x 80, the 20 nm
+    bend's design box) timed with CUDA events, against the measured bf16 peak."""
+    import torch
+
+    from warp_fdtd_b200.surrogate import Surrogate, status, train_flops
+
+    size, batch = (80, 80), 32
+    net = Surrogate(size, 8)
+    gen = torch.Generator(device="cpu").manual_seed(0)
+    x = torch.rand((batch,) + size, generator=gen).cuda()
+    T = torch.rand((batch, 8), generator=gen).cuda()
+    g = torch.randn((batch,) + size, generator=gen).cuda()
+    for _ in range(warmup):
+        net.train_step(x, T, g)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        net.train_step(x, T, g)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    flops = train_flops(size, net.base, batch)
+    peaks = ROOT / "MEASURED_PEAKS.json"
+    peak = json.loads(peaks.read_text())["bf16_tflops"] if peaks.exists() else 1590.0
+    tflops = flops / ms / 1e9
+    return {"workload": f"CNN surrogate training step, {batch} designs of {size[0]}x{size[1]}, "
+                        f"{net.count} parameters, bf16 tcgen05 GEMMs",
+            "train_step_ms": ms, "designs_per_s": batch / ms * 1e3, "tflops": tflops,
+            "peak_tflops": peak, "frac": tflops / peak, "wait_status": status()}
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -317,6 +350,11 @@ def run_ours(args, world, rank, local):
     e2e_sec = reduce_max(time.perf_counter() - t0, world)
     e2e_value = reduce_sum(float(cells * e2e_steps), world) / e2e_sec / 1e9
 
+    try:
+        surrogate = surrogate_train_rate()
+    except Exception as exc:  # the FDTD line is still reported
+        surrogate = {"error": f"{type(exc).__name__}: {exc}"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
         sample_steps = int(os.environ.get("FDTD_CPU_SAMPLE_STEPS", "60"))
@@ -349,6 +387,7 @@ def run_ours(args, world, rank, local):
             "gpu_launches": int((launches_per_step * s.steps + folds) * args.steps),
             "clocks": clock_info,
             "modal_transmission_1550nm": meas.get("modal_transmission_spectrum", [None] * 3)[2],
+            "surrogate_train": surrogate,
         }
         print(json.dumps(line), flush=True)
 

@@ -95,6 +95,22 @@ int fdtd_gather(float *q, const float *d, const float *hist, void *grad, int gra
                 const int *step, int nx, int ny, int nz, int x0, int y0, int z0, int sx,
                 int sy, int sz, int from_h, void *stream);
 
+/* One half of the reverse step, prepare + gather fused (adjoint.py:46-88 and
+ * 107-162, as sequenced by adjoint.py:388-414), bitwise the reference
+ * sequence without the d buffer.  from_h = 1: q_dst = qE, q_src = qH,
+ * magnetic scaling, H CPML state, neighbours at -1, and (with grad)
+ * grad[j] += hist[hist_step[0]] . q over the design box in float64; from_h =
+ * 0: q_dst = qH, q_src = the updated qE, electric scaling with eps, E CPML
+ * state, neighbours at +1.  The CPML state ping-pongs: psi0 is read and psi1
+ * written when step[0] is even, the other way round when odd (step is the
+ * reverse step counter, decremented once per reverse step); both start at
+ * zero.  coeff is the (3, clen, 3) table, clen >= max(nx, ny, nz). */
+int fdtd_reverse_half(int from_h, float *q_dst, const float *q_src, const float *eps,
+                      float *psi0, float *psi1, const float *coeff, int clen, const int *step,
+                      const float *hist, double *grad, const int *hist_step, int nx, int ny,
+                      int nz, float courant, int x0, int y0, int z0, int sx, int sy, int sz,
+                      void *stream);
+
 /* Replaces adjoint.py:181-223 `inject` (transpose of detector colocation):
  * source (6, count, 2) float32, weights (steps, 2); scattered with float32
  * atomics as the reference does. */
@@ -421,7 +437,8 @@ int fdtd_sg_transpose(const void *src, int lds, long long rows, int cols, void *
 int fdtd_sg_col2im(const float *dcol, int ldd, int B, int H, int W, int C, float *dx, int ldx,
                    int accumulate, void *stream);
 /* dz = bf16(y > 0 ? dy : 0) and bias_grad[c] = sum_p of the same masked values
- * (scratch: 64*C floats). */
+ * (scratch: FDTD_SG_SCRATCH_ROWS * C floats). */
+#define FDTD_SG_SCRATCH_ROWS 1024
 int fdtd_sg_relu_backward(const float *dy, int lddy, const void *y, int ldy, long long P, int C,
                           void *dz, int ldz, float *bias_grad, float *scratch, void *stream);
 /* 2 x 2 average pool of an H x W map (H, W even) and its adjoint. */
@@ -442,7 +459,7 @@ int fdtd_sg_gap_linear_backward(const float *dout, const float *feat, const floa
                                 int npix, int C, int K, float *dWl, float *dbl, float *dx,
                                 int ldx, int accumulate, void *stream);
 /* Gradient-map head: out[p] = bg + sum_c x[p, c] * wg[c]; and its reverse
- * mode (dx overwritten; scratch: 64*C floats). */
+ * mode (dx overwritten; scratch: FDTD_SG_SCRATCH_ROWS * C floats). */
 int fdtd_sg_head(const void *x, int ldx, long long P, int C, const float *wg, const float *bg,
                  float *out, void *stream);
 int fdtd_sg_head_backward(const float *dout, const void *x, int ldx, long long P, int C,

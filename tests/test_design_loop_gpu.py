@@ -55,3 +55,28 @@ def test_trained_surrogate_predicts_held_out_gradients(small):
     print(f"held-out gradient cosine {before:.3f} -> {after:.3f}; spectrum RMSE {rmse:.4f}")
     # measured on a B200: 0.03 -> 0.30 (and 0.03 -> 0.23 on the 20 nm bend)
     assert after > 0.15 and after > before + 0.15
+
+
+def test_extrapolated_loop_accepts_only_verified_improvements(small):
+    """Every surrogate-extrapolated design the loop keeps was judged by a full
+    forward against the exact T of the design it started from."""
+    from warp_fdtd_b200.design_loop import Dataset, extrapolate_loop
+    from warp_fdtd_b200.surrogate import Surrogate
+
+    problem, data, n_train = small
+    net = Surrogate(problem.shape, problem.nwav, seed=0)
+    P, T, G = data.tensors()
+    net.fit(P[:n_train], T[:n_train], G[:n_train], steps=200, batch=16, lr=1e-3)
+    run = Dataset(problem.shape, problem.nwav, g_scale=data.g_scale)
+    for i in range(n_train):
+        run.add(data.p[i], data.T[i], data.g[i])
+    p0 = np.random.default_rng(5).uniform(0, 1, problem.shape).astype(np.float32)
+    _, hist = extrapolate_loop(problem, net, p0, run, target=2.0, iters=5, step=0.1)
+    assert [h["kind"] for h in hist[::2]] == ["adjoint"] * 5
+    for before, judged in zip(hist[::2], hist[1::2]):
+        if judged["kind"] == "surrogate":
+            assert judged["T"] > before["T"]
+        else:
+            assert judged["kind"] == "rejected" and judged["T"] <= before["T"]
+    assert len(run) == n_train + 5  # each iteration's exact triple fine-tuned the network
+    print("extrapolated loop:", [(h["kind"], round(h["T"], 4)) for h in hist])

@@ -125,6 +125,8 @@ _SIGNATURES = {
     "fdtd_record_stage": [_p, _p, _p, _p, _p, _p, _i, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i,
                           _i, _i, _i, _p],
     "fdtd_dft_fold": [_p, _p, _i, _p, _i, _p, _i, _p, _ll, _p],
+    "fdtd_reverse_half": [_i, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p, _p, _i, _i, _i, _f, _i,
+                          _i, _i, _i, _i, _i, _p],
     "fdtd_sg_gemm": [ctypes.POINTER(SgGemmArgs), _p],
     "fdtd_sg_gemm_splits": [ctypes.POINTER(SgGemmArgs)],
     "fdtd_sg_status": [ctypes.POINTER(_i), _i],

@@ -34,7 +34,7 @@ from .solver import Solver, cpml_coefficients
 
 class Adjoint(Solver):
     def __init__(self, case, box=None, checkpoint_every=256, strict=False, device="cuda:0",
-                 graph_steps=64, material_kwargs=None):
+                 graph_steps=64, material_kwargs=None, fused_reverse=True):
         super().__init__(case, device=device, graph_steps=graph_steps, material="f32")
         settings = self.meta["settings"]
         if strict:
@@ -76,6 +76,10 @@ class Adjoint(Solver):
         self.psie = torch.zeros((6, n), **f32)
         self.psih = torch.zeros((6, n), **f32)
         self.d = torch.empty((6, n), **f32)
+        # fused reverse halves (fdtd_reverse_half): the CPML state ping-pongs
+        self.fused_reverse = bool(fused_reverse)
+        self.psie2 = torch.zeros((6, n), **f32) if self.fused_reverse else None
+        self.psih2 = torch.zeros((6, n), **f32) if self.fused_reverse else None
         self.grad = torch.zeros(self.design_n, dtype=torch.float64, device=dev)
         self.reverse_step = torch.zeros(1, dtype=torch.int32, device=dev)
         self.hist_step = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -197,8 +201,24 @@ class Adjoint(Solver):
 
     def reverse_one(self):
         """adjoint.py:388-414 with the float64 gradient and a segment-relative
-        history index."""
+        history index.  With fused_reverse each prepare + gather pair is one
+        pass (fdtd_reverse_half), bitwise the same values."""
         self.inject(0)
+        if self.fused_reverse:
+            stream = _lib.stream_handle(self.device)
+            clen = int(self._coeff3["H"].shape[1])
+            _lib.call("fdtd_reverse_half", 1, ptr(self.qe), ptr(self.qh), ptr(self.eps),
+                      ptr(self.psih), ptr(self.psih2), ptr(self._coeff3["H"]), clen,
+                      ptr(self.reverse_step), ptr(self.history), ptr(self.grad),
+                      ptr(self.hist_step), *self.shape, self.courant, *self.box, stream)
+            _lib.call("fdtd_reverse_half", 0, ptr(self.qh), ptr(self.qe), ptr(self.eps),
+                      ptr(self.psie), ptr(self.psie2), ptr(self._coeff3["E"]), clen,
+                      ptr(self.reverse_step), None, None, None, *self.shape, self.courant,
+                      0, 0, 0, 0, 0, 0, stream)
+            self.inject(1)
+            _lib.call("fdtd_advance", ptr(self.reverse_step), -1, stream)
+            _lib.call("fdtd_advance", ptr(self.hist_step), -1, stream)
+            return
         common = [*self.shape, self.courant]
         kernels.prepare(self.qh, self.eps, self.psih, self._coeff3["H"], self.d, *common, 0)
         args = [self.d, self.history, self.grad, self.hist_step, *self.shape, *self.box]
@@ -211,8 +231,9 @@ class Adjoint(Solver):
         _lib.call("fdtd_advance", ptr(self.hist_step), -1, stream)
 
     def reset_reverse(self):
-        for a in (self.qe, self.qh, self.psie, self.psih, self.grad):
-            a.zero_()
+        for a in (self.qe, self.qh, self.psie, self.psih, self.grad, self.psie2, self.psih2):
+            if a is not None:
+                a.zero_()
         self.reverse_step.fill_(self.steps - 1)
         torch.cuda.synchronize(self.device)
 

@@ -851,7 +851,13 @@ int fdtd_sg_col2im(const float *dcol, int ldd, int B, int H, int W, int C, float
     return launch_status("fdtd_sg_col2im");
 }
 
-#define SG_GROUPS 64
+// Row groups of the two-stage column reductions: one group per 256 rows, at
+// most SG_GROUPS_MAX (the scratch holds SG_GROUPS_MAX * C floats).
+#define SG_GROUPS_MAX 1024
+static int sg_groups(long long P) {
+    long long g = (P + 255) / 256;
+    return (int)(g < 1 ? 1 : (g > SG_GROUPS_MAX ? SG_GROUPS_MAX : g));
+}
 
 int fdtd_sg_relu_backward(const float *dy, int lddy, const void *y, int ldy, long long P, int C,
                           void *dz, int ldz, float *bias_grad, float *scratch, void *stream) {
@@ -860,11 +866,11 @@ int fdtd_sg_relu_backward(const float *dy, int lddy, const void *y, int ldy, lon
         set_error("fdtd_sg_relu_backward: bad argument");
         return FDTD_ERR_ARG;
     }
-    dim3 grid((C + 31) / 32, SG_GROUPS);
+    const int G = sg_groups(P);
+    dim3 grid((C + 31) / 32, G);
     relu_backward_kernel<<<grid, dim3(32, 8), 0, st(stream)>>>(
-        dy, lddy, (const bf16 *)y, ldy, P, C, (bf16 *)dz, ldz, scratch, SG_GROUPS);
-    colsum_final_kernel<<<nblocks(C, 128), 128, 0, st(stream)>>>(scratch, SG_GROUPS, C,
-                                                                 bias_grad);
+        dy, lddy, (const bf16 *)y, ldy, P, C, (bf16 *)dz, ldz, scratch, G);
+    colsum_final_kernel<<<nblocks(C, 128), 128, 0, st(stream)>>>(scratch, G, C, bias_grad);
     return launch_status("fdtd_sg_relu_backward");
 }
 
@@ -965,13 +971,13 @@ int fdtd_sg_head_backward(const float *dout, const void *x, int ldx, long long P
         return FDTD_ERR_ARG;
     }
     cudaStream_t s = st(stream);
+    const int G = sg_groups(P);
     head_dgrad_kernel<<<nblocks(P * C, 256), 256, 0, s>>>(dout, P, C, wg, dx, lddx);
-    rowdot_kernel<<<dim3((C + 31) / 32, SG_GROUPS), dim3(32, 8), 0, s>>>(
-        dout, (const bf16 *)x, ldx, P, C, scratch, SG_GROUPS);
-    colsum_final_kernel<<<nblocks(C, 128), 128, 0, s>>>(scratch, SG_GROUPS, C, dwg);
-    rowdot_kernel<<<dim3(1, SG_GROUPS), dim3(32, 8), 0, s>>>(dout, nullptr, 0, P, 1, scratch,
-                                                             SG_GROUPS);
-    colsum_final_kernel<<<1, 128, 0, s>>>(scratch, SG_GROUPS, 1, dbg);
+    rowdot_kernel<<<dim3((C + 31) / 32, G), dim3(32, 8), 0, s>>>(dout, (const bf16 *)x, ldx, P,
+                                                                  C, scratch, G);
+    colsum_final_kernel<<<nblocks(C, 128), 128, 0, s>>>(scratch, G, C, dwg);
+    rowdot_kernel<<<dim3(1, G), dim3(32, 8), 0, s>>>(dout, nullptr, 0, P, 1, scratch, G);
+    colsum_final_kernel<<<1, 128, 0, s>>>(scratch, G, 1, dbg);
     return launch_status("fdtd_sg_head_backward");
 }
 

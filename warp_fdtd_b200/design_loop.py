@@ -13,7 +13,11 @@ p <- clip(p + step * d / max|d|, 0, 1):
 * plain adjoint loop: d = dT/dp from Adjoint.differentiate (one forward and
   one checkpointed reverse sweep per iteration); T of each iterate comes from
   the same call.
-* surrogate-proposed loop: d = the CNN's predicted gradient map at p.  The
+* surrogate-extrapolated loop (extrapolate_loop): each iteration is the
+  adjoint step from p followed by k steps along the CNN's predicted gradient
+  map; a full FDTD forward accepts the extrapolated design only if its T
+  beats T(p), otherwise the loop keeps the plain adjoint step.
+* surrogate-proposed loop (surrogate_loop): d = the CNN's predicted gradient map at p.  The
   proposal q is judged by a full FDTD forward and accepted only if T(q) > T(p).
   On rejection the loop falls back to the exact method: differentiate at p,
   take the adjoint step, measure T of the result with a full forward, and
@@ -190,6 +194,40 @@ def surrogate_loop(problem, net, p0, data, target=0.9, iters=100, step=0.1, fine
     return p, hist
 
 
+def extrapolate_loop(problem, net, p0, data, target=0.9, iters=100, step=0.1, k=1,
+                     finetune_steps=15, lr=3e-4, window=64):
+    """Surrogate-extrapolated adjoint loop; returns (p, history).
+
+    Each iteration differentiates at the current design p (exact T and dT/dp;
+    the triple fine-tunes the surrogate) and takes the adjoint step to p1; the
+    surrogate then extrapolates k more steps along its predicted gradient, and
+    a full FDTD forward judges the result q: accepted when T(q) > T(p), else
+    the loop continues from p1 exactly as the plain adjoint loop would."""
+    p = np.asarray(p0, np.float32).copy()
+    hist = []
+    t0 = time.perf_counter()
+    for it in range(iters):
+        T, spectrum, g = problem.differentiate(p)
+        hist.append(dict(it=it, T=T, t=time.perf_counter() - t0, kind="adjoint"))
+        if T >= target:
+            break
+        data.add(p, spectrum, g)
+        finetune(net, data, finetune_steps, lr, window, seed=it)
+        p1 = ascent(p, g, step)
+        q = p1
+        for _ in range(k):
+            _, ghat = net.predict(torch.from_numpy(q).to(net.device))
+            q = ascent(q, ghat.cpu().numpy(), step)
+        Tq, _ = problem.transmission(q)
+        accepted = Tq > T
+        hist.append(dict(it=it, T=Tq, t=time.perf_counter() - t0,
+                         kind="surrogate" if accepted else "rejected"))
+        if accepted and Tq >= target:
+            break
+        p = q if accepted else p1
+    return p, hist
+
+
 def finetune(net, data, steps, lr, window, newest=8, batch=32, seed=0):
     """Adam steps on minibatches that always hold the newest triple (`newest`
     copies) next to random triples of the last `window`: the surrogate follows
@@ -204,8 +242,10 @@ def finetune(net, data, steps, lr, window, newest=8, batch=32, seed=0):
 
 
 def time_to(hist, target):
+    """Time of the first verified design with T >= target (rejected proposals
+    are not designs the loop holds)."""
     for h in hist:
-        if h["T"] >= target:
+        if h["T"] >= target and h["kind"] != "rejected":
             return h["t"]
     return None
 
@@ -223,36 +263,37 @@ def held_out_cosine(net, data, idx):
     return float(np.mean(out))
 
 
-def run(case, box=None, target=0.9, iters=100, step=0.1, train_seeds=range(1, 9),
-        traj_steps=16, held_out_seeds=(100,), held_out_steps=8, train_steps=1500, batch=32, lr=1e-3,
-        finetune_steps=30, seed=0, device="cuda:0", log=print, data_path=None,
-        save_data=None):
-    """Data generation (or a saved data set), training, then both loops from
-    the same seeded start."""
+def run(case, box=None, target=0.9, iters=100, steps=(0.1,), starts=(0,),
+        train_seeds=range(1, 9), traj_steps=16, held_out_seeds=(100,), held_out_steps=8,
+        train_steps=1500, batch=32, lr=1e-3, finetune_steps=30, data_step=0.1, device="cuda:0",
+        log=print, data_path=None, save_data=None,
+        loops=("adjoint", "extrapolate", "propose")):
+    """Data generation (or a saved data set), training, then every loop at
+    every step size from every seeded start (uniform densities of seed s).
+    Each surrogate loop starts from the same trained network and data set."""
     problem = DesignProblem(case, box=box, device=device)
     shape = problem.shape
-    p_start = np.random.default_rng(seed).uniform(0, 1, shape).astype(np.float32)
     # warm-up: CUDA graphs of the forward and reverse sweeps
-    problem.differentiate(p_start)
+    problem.differentiate(np.full(shape, 0.5, np.float32))
     torch.cuda.synchronize()
-    res = dict(case=str(case), shape=list(problem.adj.shape), steps=problem.adj.steps,
-               design=list(shape), target=target, step=step, iters=iters)
+    res = dict(case=str(case), shape=list(problem.adj.shape), time_steps=problem.adj.steps,
+               design=list(shape), target=target, iters=iters, runs={})
 
     t0 = time.perf_counter()
     if data_path:
         data, n_train = Dataset.load(data_path, device)
         res["data_from"] = str(data_path)
     else:
-        data = generate(problem, list(train_seeds), traj_steps, step)
+        data = generate(problem, list(train_seeds), traj_steps, data_step)
         n_train = len(data)
-        generate(problem, list(held_out_seeds), held_out_steps, step, data)
+        generate(problem, list(held_out_seeds), held_out_steps, data_step, data)
         if save_data:
             data.save(save_data, n_train)
     res["data_seconds"] = time.perf_counter() - t0
     res["train_triples"], res["held_out_triples"] = n_train, len(data) - n_train
     log(f"data: {len(data)} triples in {res['data_seconds']:.1f} s")
 
-    net = Surrogate(shape, problem.nwav, device=device, seed=seed)
+    net = Surrogate(shape, problem.nwav, device=device, seed=0)
     held = list(range(n_train, len(data)))
     res["held_out_cosine_untrained"] = held_out_cosine(net, data, held)
     P, T, G = data.tensors()
@@ -268,24 +309,38 @@ def run(case, box=None, target=0.9, iters=100, step=0.1, train_seeds=range(1, 9)
     log(f"trained in {res['train_seconds']:.1f} s; held-out gradient cosine "
         f"{res['held_out_cosine_untrained']:.3f} -> {res['held_out_cosine_trained']:.3f}")
 
-    problem.forwards = problem.adjoints = 0
-    _, h_adj = adjoint_loop(problem, p_start, target, iters, step)
-    res["adjoint"] = dict(history=h_adj, time_to_target=time_to(h_adj, target),
-                          best=max(h["T"] for h in h_adj), forwards=problem.forwards,
-                          adjoints=problem.adjoints)
-    log(f"adjoint loop: best T {res['adjoint']['best']:.4f}, time to {target}: "
-        f"{res['adjoint']['time_to_target']}")
-    problem.forwards = problem.adjoints = 0
-    _, h_sur = surrogate_loop(problem, net, p_start, data, target, iters, step, finetune_steps)
-    res["surrogate"] = dict(history=h_sur, time_to_target=time_to(h_sur, target),
-                            best=max(h["T"] for h in h_sur), forwards=problem.forwards,
-                            adjoints=problem.adjoints,
-                            accepted=sum(h["kind"] == "surrogate" for h in h_sur))
-    for k in ("adjoint", "surrogate"):
-        res[k]["time_to"] = {str(v): time_to(res[k]["history"], v)
-                             for v in (0.3, 0.5, 0.7, 0.8, 0.9) if v <= target}
-    log(f"surrogate loop: best T {res['surrogate']['best']:.4f}, time to {target}: "
-        f"{res['surrogate']['time_to_target']}, accepted {res['surrogate']['accepted']}")
+    trained = net.params_numpy()
+    for start in starts:
+        p_start = np.random.default_rng(start).uniform(0, 1, shape).astype(np.float32)
+        for step in steps:
+            for name in loops:
+                problem.forwards = problem.adjoints = 0
+                if name == "adjoint":
+                    _, h = adjoint_loop(problem, p_start, target, iters, step)
+                else:
+                    run_net = Surrogate(shape, problem.nwav, device=device, params=trained)
+                    run_data = Dataset(shape, problem.nwav, device, data.g_scale)
+                    for i in range(n_train):
+                        run_data.add(data.p[i], data.T[i], data.g[i])
+                    if name == "extrapolate":
+                        _, h = extrapolate_loop(problem, run_net, p_start, run_data, target,
+                                                iters, step, k=1)
+                    elif name == "propose":
+                        _, h = surrogate_loop(problem, run_net, p_start, run_data, target, iters,
+                                              step, finetune_steps)
+                    else:
+                        raise ValueError(f"unknown loop {name!r}")
+                key = f"{name}_step{step}_start{start}"
+                res["runs"][key] = dict(
+                    loop=name, step=step, start=start, history=h,
+                    time_to_target=time_to(h, target),
+                    best=max(x["T"] for x in h if x["kind"] != "rejected"),
+                    forwards=problem.forwards, adjoints=problem.adjoints,
+                    accepted=sum(x["kind"] == "surrogate" for x in h))
+                r = res["runs"][key]
+                log(f"{key}: time to {target} {r['time_to_target']}, best T {r['best']:.4f}, "
+                    f"{r['adjoints']} adjoint + {r['forwards']} forward runs, "
+                    f"{r['accepted']} surrogate steps kept")
     return res
 
 
@@ -295,27 +350,30 @@ def main(argv=None):
     ap.add_argument("--box", type=int, nargs=6, default=None)
     ap.add_argument("--target", type=float, default=0.9)
     ap.add_argument("--iters", type=int, default=100)
-    ap.add_argument("--step", type=float, default=0.1)
+    ap.add_argument("--steps", type=float, nargs="+", default=[0.1],
+                    help="ascent step sizes (max-norm) to run every loop at")
+    ap.add_argument("--starts", type=int, nargs="+", default=[0],
+                    help="seeds of the uniform-density starting designs")
     ap.add_argument("--train-seeds", type=int, default=8)
     ap.add_argument("--traj-steps", type=int, default=16)
     ap.add_argument("--held-out-steps", type=int, default=8)
     ap.add_argument("--train-steps", type=int, default=1500)
-    ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=None)
     ap.add_argument("--data", default=None, help="saved data set (Dataset.save) to train on")
     ap.add_argument("--save-data", default=None)
+    ap.add_argument("--loops", nargs="+", default=["adjoint", "extrapolate", "propose"],
+                    choices=["adjoint", "extrapolate", "propose"])
     a = ap.parse_args(argv)
-    res = run(a.case, a.box, a.target, a.iters, a.step, range(1, 1 + a.train_seeds),
-              a.traj_steps, held_out_steps=a.held_out_steps, train_steps=a.train_steps,
-              seed=a.seed, data_path=a.data, save_data=a.save_data)
-    text = json.dumps(res)
+    res = run(a.case, a.box, a.target, a.iters, tuple(a.steps), tuple(a.starts),
+              range(1, 1 + a.train_seeds), a.traj_steps, held_out_steps=a.held_out_steps,
+              train_steps=a.train_steps, data_path=a.data, save_data=a.save_data,
+              loops=a.loops)
     if a.out:
         with open(a.out, "w") as f:
-            f.write(text)
-    print(json.dumps({k: v for k, v in res.items() if k not in ("adjoint", "surrogate",
-                                                                 "train_loss")}))
-    print(json.dumps({k: {kk: vv for kk, vv in res[k].items() if kk != "history"}
-                      for k in ("adjoint", "surrogate")}))
+            json.dump(res, f)
+    print(json.dumps({k: v for k, v in res.items() if k not in ("runs", "train_loss")}))
+    print(json.dumps({k: {kk: vv for kk, vv in r.items() if kk != "history"}
+                      for k, r in res["runs"].items()}))
 
 
 if __name__ == "__main__":

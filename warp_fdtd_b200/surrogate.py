@@ -30,7 +30,7 @@ from ._lib import SgGemmArgs
 
 BF16 = torch.bfloat16
 F32 = torch.float32
-SCRATCH_GROUPS = 64  # fdtd_sg_relu_backward / head_backward reduction groups
+SCRATCH_ROWS = 1024  # FDTD_SG_SCRATCH_ROWS: partial-sum rows of the column reductions
 
 
 def architecture(base=32):
@@ -209,7 +209,7 @@ class Surrogate:
             self._splits[(name, B)] = s
             part = max(part, s * 9 * cin * cout)
         b["part"] = f(part)
-        b["scratch"] = f(SCRATCH_GROUPS * max(c[3], 1))
+        b["scratch"] = f(SCRATCH_ROWS * max(c[3], 1))
         b["loss_T"] = f((B * self.nwav + 255) // 256)
         b["loss_g"] = f((P[0] + 255) // 256)
         self._bufs[B] = b
@@ -430,3 +430,54 @@ def default_init(seed=0, base=32, nwav=8):
     p["ghead.w"] = (rng.standard_normal(base) / np.sqrt(base)).astype(np.float32)
     p["ghead.b"] = np.zeros(1, np.float32)
     return p
+
+
+def train_flops(size, base=32, batch=1):
+    """Algorithmic FLOPs of one training step (forward, input and weight
+    gradients of every 3 x 3 convolution, 2 per multiply-add; the layer
+    without an input gradient counted once less), for `batch` designs."""
+    H, W = size
+    total = 0
+    for name, cin, cout, lev in architecture(base):
+        mac = batch * (H >> lev) * (W >> lev) * 9 * cin * cout
+        total += 2 * mac * (2 if name == "e0a" else 3)
+    return total
+
+
+def main(argv=None):
+    """Time training steps of the surrogate on synthetic designs:
+    python -m warp_fdtd_b200.surrogate [--batch 32] [--size 80 80] [--steps 50]"""
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description=main.__doc__)
+    ap.add_argument("--batch", type=int, default=32)
+    ap.add_argument("--size", type=int, nargs=2, default=(80, 80))
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    a = ap.parse_args(argv)
+    size = tuple(a.size)
+    net = Surrogate(size, 8)
+    gen = torch.Generator(device="cpu").manual_seed(0)
+    x = torch.rand((a.batch,) + size, generator=gen).cuda()
+    T = torch.rand((a.batch, 8), generator=gen).cuda()
+    g = torch.randn((a.batch,) + size, generator=gen).cuda()
+    for _ in range(a.warmup):
+        net.train_step(x, T, g)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.steps):
+        net.train_step(x, T, g)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / a.steps
+    flops = train_flops(size, net.base, a.batch)
+    print(json.dumps(dict(workload=f"surrogate_train_{size[0]}x{size[1]}_b{a.batch}",
+                          train_step_ms=ms, designs_per_s=a.batch / ms * 1e3,
+                          tflops=flops / ms / 1e9, flops_per_step=flops,
+                          params=net.count, wait_status=status())))
+
+
+if __name__ == "__main__":
+    main()
