@@ -678,14 +678,21 @@ template <int BN, bool SW>
 static int launch_gemm(const fdtd_sg_gemm_args *g, int splits, int per, int nchunks,
                        cudaStream_t stream) {
     using CF = GemmCfg<BN>;
-    static std::once_flag once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(once, [] {
-        attr_err = cudaFuncSetAttribute(gemm_kernel<BN, SW>,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM);
-    });
-    if (attr_err != cudaSuccess) {
-        set_error("fdtd_sg_gemm: %s", cudaGetErrorString(attr_err));
+    // the shared-memory opt-in is per device: set it once on each
+    static std::mutex mu;
+    static bool ready[64] = {};
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err == cudaSuccess) {
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev < 0 || dev >= 64 || !ready[dev]) {
+            err = cudaFuncSetAttribute(gemm_kernel<BN, SW>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, CF::SMEM);
+            if (err == cudaSuccess && dev >= 0 && dev < 64) ready[dev] = true;
+        }
+    }
+    if (err != cudaSuccess) {
+        set_error("fdtd_sg_gemm: %s", cudaGetErrorString(err));
         return FDTD_ERR_CUDA;
     }
     CUtensorMap ta, tb;

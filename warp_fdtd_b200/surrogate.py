@@ -76,7 +76,7 @@ def gemm(A, B, C, M, N, K, lda, ldb, ldc, bias=None, relu=False, accumulate=Fals
     a.splits, a.split_stride = splits, split_stride
     a.accumulate, a.relu, a.layout = int(accumulate), int(relu), int(layout)
     _lib.call("fdtd_sg_gemm", ctypes.byref(a), _s(stream))
-    return _lib.load().fdtd_sg_gemm_splits(ctypes.byref(a))
+    return _lib.load().fdtd_sg_gemm_splits(ctypes.byref(a)) if splits > 1 else 1
 
 
 def gemm_splits(M, N, K, splits):
