@@ -67,6 +67,10 @@ class Adjoint(Solver):
         K = min(K, self.steps)
         K += K & 1  # even: checkpoints land on parity-0 buffers
         self.checkpoint_every = K
+        # one segment: the forward itself records the history, so the reverse
+        # sweep needs no recomputation (the reference's storage scheme)
+        self.history_in_forward = K >= self.steps
+        self._history_fresh = False
         dev = self.device
         f32 = dict(dtype=torch.float32, device=dev)
         n = self.n
@@ -99,13 +103,25 @@ class Adjoint(Solver):
         for dst, src in zip((self._E[0], self._H[0], self._psi_e[0], self._psi_h[0]), snap):
             dst.copy_(src)
 
+    def _after_update(self, stream):
+        if self.history_in_forward:
+            x0, y0, z0, sx, sy, sz = self.box
+            _lib.call("fdtd_record_curl_pp", ptr(self._H[0]), ptr(self._H[1]), self._pitch,
+                      ptr(self.step), ptr(self.hist_step), ptr(self.history), *self.shape, x0,
+                      y0, z0, sx, sy, sz, float(self.courant), stream)
+            _lib.call("fdtd_advance", ptr(self.hist_step), 1, stream)
+
     def run(self):
         """Forward trajectory with detectors, saving a state checkpoint every
-        `checkpoint_every` steps (at step counts that are multiples of it)."""
+        `checkpoint_every` steps (at step counts that are multiples of it);
+        with a single segment the design-box history is recorded instead."""
         K = self.checkpoint_every
         self.checkpoints = {}
+        self._history_fresh = False
+        if self.history_in_forward:
+            self.hist_step.fill_(self._issued)
         with torch.cuda.device(self.device):
-            if self.graphs and K % self.graph_steps == 0:
+            if self.graphs and (K % self.graph_steps == 0 or self.history_in_forward):
                 for c in range(self.steps // self.graph_steps):
                     start = c * self.graph_steps
                     if start % K == 0 and start > 0:
@@ -125,6 +141,7 @@ class Adjoint(Solver):
                     if self._issued % K == 0 and self._issued > 0:
                         self.checkpoints[self._issued] = self._snapshot()
                     self.launch_step()
+            self._history_fresh = self.history_in_forward
             torch.cuda.synchronize(self.device)
 
     def _recompute_step(self, stream):
@@ -264,7 +281,8 @@ class Adjoint(Solver):
         """Reverse sweep over all segments, last first."""
         with torch.cuda.device(self.device):
             for start, length in reversed(self._segments()):
-                self._recompute(start, length)
+                if not (self._history_fresh and start == 0 and length == self.steps):
+                    self._recompute(start, length)
                 self.reverse_step.fill_(start + length - 1)
                 self.hist_step.fill_(length - 1)
                 g = self.reverse_graphs.get(length)
@@ -273,6 +291,7 @@ class Adjoint(Solver):
                         self.reverse_one()
                 else:
                     g.replay()
+            self._history_fresh = False
             torch.cuda.synchronize(self.device)
 
     # ------------------------------------------------------------ design

@@ -61,11 +61,13 @@ __global__ void reverse_half_kernel(float *__restrict__ q_dst, const float *__re
                                     int sz) {
     constexpr bool ELECTRIC = !FROM_H;
     const i64 n = (i64)nx * ny * nz;
-    const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int x = (int)(i / ((i64)ny * nz));
-    const int y = (int)((i / nz) % ny);
-    const int z = (int)(i % nz);
+    // one x plane per grid row: 32-bit (y, z) decomposition within the plane
+    const int x = blockIdx.y;
+    const int yz = blockIdx.x * blockDim.x + threadIdx.x;
+    if (yz >= ny * nz) return;
+    const int y = yz / nz;
+    const int z = yz - y * nz;
+    const i64 i = (i64)x * ny * nz + yz;
     const int s = step[0] & 1;
     const float *psi_in = s ? psi1 : psi0;
     float *psi_out = s ? psi0 : psi1;
@@ -128,7 +130,11 @@ extern "C" int fdtd_reverse_half(int from_h, float *q_dst, const float *q_src, c
         set_error("fdtd_reverse_half: invalid arguments");
         return FDTD_ERR_ARG;
     }
-    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (nx > 65535 || (i64)ny * nz > 0x7fffffffLL) {
+        set_error("fdtd_reverse_half: nx <= 65535 and ny*nz < 2^31 required");
+        return FDTD_ERR_ARG;
+    }
+    const dim3 blocks((unsigned)(((i64)ny * nz + 255) / 256), (unsigned)nx);
     cudaStream_t s = (cudaStream_t)stream;
     if (from_h)
         reverse_half_kernel<true><<<blocks, 256, 0, s>>>(q_dst, q_src, eps, psi0, psi1, coeff,

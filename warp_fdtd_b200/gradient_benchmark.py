@@ -20,8 +20,10 @@ gradient_benchmark.py:16-165 --
 benchmark (324 x 324 x 144 cells, 4000 steps).  The 125 x 125 x 11 design box
 sits over the arc.  Densities are seeded uniform in [0, 1]; the material map
 is a 19 x 19 Gaussian filter (sigma 3 cells = 60 nm), tanh projection
-beta = 8, and eps linear from 2.085 to 12.11.  Checkpoints every 256 steps;
-the gradient is checked against central differences (h = 1e-3) on 16 seeded
+beta = 8, and eps linear from 2.085 to 12.11.  Checkpoints every 256 steps
+(`--checkpoint-every`; at or above the step count the forward records the
+whole design-box history and the reverse sweep recomputes nothing); the
+gradient is checked against central differences (h = 1e-3) on 16 seeded
 pixels from the upper quartile of |gradient|.
 
     python -m warp_fdtd_b200.gradient_benchmark [--case DIR] [--reps 2] [--out result.json]
@@ -80,9 +82,9 @@ def _timed(adj, reps):
     return out
 
 
-def reference_case(case, reps=2):
+def reference_case(case, reps=2, checkpoint_every=256):
     case = Path(case)
-    adj = Adjoint(case, checkpoint_every=256)
+    adj = Adjoint(case, checkpoint_every=checkpoint_every)
     attach(adj)
     p0 = np.asarray(adj.data["parameters/p0"])[..., 0]
     x0, y0, z0, sx, sy, sz = adj.box
@@ -138,14 +140,15 @@ def reference_case(case, reps=2):
     return res
 
 
-def config3(reps=1, workdir=None, pixels=16, h=1e-3):
+def config3(reps=1, workdir=None, pixels=16, h=1e-3, checkpoint_every=256):
     from . import scene
 
     workdir = Path(workdir or tempfile.mkdtemp(prefix="wfb_config3_"))
     case = scene.bend_case(workdir / "bend20", steps=4000)
     box = (145, 54, 67, 125, 125, 11)
     material_kwargs = dict(beta=8.0, eps_lo=2.085, contrast=12.11 - 2.085, radius=9, sigma=3.0)
-    adj = Adjoint(case, box=box, checkpoint_every=256, material_kwargs=material_kwargs)
+    adj = Adjoint(case, box=box, checkpoint_every=checkpoint_every,
+                  material_kwargs=material_kwargs)
     attach(adj)
     p = np.random.default_rng(0).uniform(0, 1, (125, 125)).astype(np.float32)
     loss, grad = adj.differentiate(p)
@@ -155,7 +158,8 @@ def config3(reps=1, workdir=None, pixels=16, h=1e-3):
                seconds=[t[0] for t in times], forward_seconds=[t[1] for t in times],
                backward_seconds=[t[2] for t in times],
                cell_updates=int(np.prod(adj.shape)) * adj.steps,
-               history_bytes=int(adj.history.numel() * 4))
+               history_bytes=int(adj.history.numel() * 4),
+               checkpoint_every=adj.checkpoint_every)
     g = np.asarray(grad, np.float64).ravel()
     rng = np.random.default_rng(16)
     top = np.flatnonzero(np.abs(g) >= np.quantile(np.abs(g), 0.75))
@@ -182,11 +186,15 @@ def main(argv=None):
                                           "golden" / "gradient20"))
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--config3", action="store_true")
+    ap.add_argument("--checkpoint-every", type=int, default=256,
+                    help="steps per checkpoint segment; >= the step count keeps the whole "
+                         "design-box history and skips the recomputation")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     if a.reps < 1:
         ap.error("--reps must be positive")
-    res = config3(reps=a.reps) if a.config3 else reference_case(a.case, a.reps)
+    res = (config3(reps=a.reps, checkpoint_every=a.checkpoint_every) if a.config3
+           else reference_case(a.case, a.reps, a.checkpoint_every))
     text = json.dumps(res, indent=2)
     if a.out:
         Path(a.out).write_text(text + "\n")

@@ -523,6 +523,7 @@ class Solver:
             raise ValueError("Trajectory complete; call reset() before stepping again")
         stream = _lib.stream_handle(self.device)
         _lib.call("fdtd_step_fused", self._args, stream)
+        self._after_update(stream)
         planes, grouped = self._staged_planes()
         for monitor in self.monitors:
             if id(monitor) not in grouped:
@@ -541,6 +542,11 @@ class Solver:
             if monitor.is_phasor and (self._issued % monitor.batch == 0
                                       or self._issued == self.steps):
                 monitor.fold(self, self._issued)
+
+    def _after_update(self, stream):
+        """Hook between the fused update and the detectors (the step counter
+        not yet advanced); the adjoint driver records its design-box history
+        here when it keeps the whole trajectory."""
 
     def _staged_planes(self):
         """The staged phasor monitors that share one recording launch: two to
