@@ -231,7 +231,7 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def surrogate_train_rate(steps=20, warmup=3):
+def surrogate_train_rate(steps=20, warmup=3, device="cuda:0"):
     """The CNN surrogate's training step (32 designs of 80 x 80, the 20 nm
     bend's design box) timed with CUDA events, against the measured bf16 peak."""
     import torch
@@ -239,11 +239,11 @@ def surrogate_train_rate(steps=20, warmup=3):
     from warp_fdtd_b200.surrogate import Surrogate, status, train_flops
 
     size, batch = (80, 80), 32
-    net = Surrogate(size, 8)
+    net = Surrogate(size, 8, device=device)
     gen = torch.Generator(device="cpu").manual_seed(0)
-    x = torch.rand((batch,) + size, generator=gen).cuda()
-    T = torch.rand((batch, 8), generator=gen).cuda()
-    g = torch.randn((batch,) + size, generator=gen).cuda()
+    x = torch.rand((batch,) + size, generator=gen).to(device)
+    T = torch.rand((batch, 8), generator=gen).to(device)
+    g = torch.randn((batch,) + size, generator=gen).to(device)
     for _ in range(warmup):
         net.train_step(x, T, g)
     torch.cuda.synchronize()
@@ -272,7 +272,7 @@ def run_ours(args, world, rank, local):
     from warp_fdtd_b200.solver import Solver
 
     case = make_bundle(args.workload, args.time_steps)
-    s = Solver(case, graph_steps=64)
+    s = Solver(case, device=f"cuda:{local}", graph_steps=64)
     attach(s)
     s.compile()
     stream = torch.cuda.current_stream()
@@ -351,7 +351,7 @@ def run_ours(args, world, rank, local):
     e2e_value = reduce_sum(float(cells * e2e_steps), world) / e2e_sec / 1e9
 
     try:
-        surrogate = surrogate_train_rate()
+        surrogate = surrogate_train_rate(device=f"cuda:{local}")
     except Exception as exc:  # the FDTD line is still reported
         surrogate = {"error": f"{type(exc).__name__}: {exc}"}
 

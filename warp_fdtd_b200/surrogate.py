@@ -158,6 +158,10 @@ class Surrogate:
         return {name: self.view(name, self.grads).cpu().numpy().copy() for name in self.slots}
 
     def _cast(self, stream=None):
+        with torch.cuda.device(self.device):
+            self._cast_launch(stream)
+
+    def _cast_launch(self, stream=None):
         for name, cin, cout, _ in self.convs:
             _lib.call("fdtd_sg_cast_weights", ptr(self.view(name + ".w")), cout, 9 * cin,
                       ptr(self.wb[name]), self.wb[name].shape[1], ptr(self.wt[name]), _s(stream))
@@ -235,6 +239,10 @@ class Surrogate:
     def forward(self, density, stream=None):
         """density (B, H, W) float32 on the device -> (T (B, nwav), g (B, H, W)),
         float32 views of internal buffers (valid until the next call)."""
+        with torch.cuda.device(self.device):
+            return self._forward(density, stream)
+
+    def _forward(self, density, stream=None):
         if density.shape[1:] != (self.H, self.W):
             raise ValueError(f"expected (B, {self.H}, {self.W}) densities")
         density = density.to(device=self.device, dtype=F32).contiguous()
@@ -315,6 +323,10 @@ class Surrogate:
     def backward(self, dT=None, dg=None, stream=None):
         """Parameter gradients (into self.grads) of sum(dT * T) + sum(dg * g) for
         the last forward; dT, dg default to the loss gradients left by loss()."""
+        with torch.cuda.device(self.device):
+            return self._backward(dT, dg, stream)
+
+    def _backward(self, dT=None, dg=None, stream=None):
         B = self._last_B
         b = self._bufs[B]
         if dT is not None:
@@ -369,21 +381,26 @@ class Surrogate:
         tensors (B, nwav) and (B, H, W)); leaves the output gradients for
         backward().  Returns the loss as a float (one device sync) when value."""
         b = self._bufs[self._last_B]
-        s = _s(stream)
-        nT, ng = b["T"].numel(), b["g"].numel()
-        _lib.call("fdtd_sg_mse", ptr(b["T"]), ptr(T_target.contiguous()), nT, w_T / nT,
-                  ptr(b["dT"]), ptr(b["loss_T"]), s)
-        _lib.call("fdtd_sg_mse", ptr(b["g"]), ptr(g_target.contiguous()), ng, w_g / ng,
-                  ptr(b["dg"]), ptr(b["loss_g"]), s)
+        with torch.cuda.device(self.device):
+            s = _s(stream)
+            nT, ng = b["T"].numel(), b["g"].numel()
+            self._loss_launch(b, s, T_target, g_target, w_T, w_g, nT, ng)
         if not value:
             return None
         return float(w_T * b["loss_T"].sum().item() / nT + w_g * b["loss_g"].sum().item() / ng)
 
+    def _loss_launch(self, b, s, T_target, g_target, w_T, w_g, nT, ng):
+        _lib.call("fdtd_sg_mse", ptr(b["T"]), ptr(T_target.contiguous()), nT, w_T / nT,
+                  ptr(b["dT"]), ptr(b["loss_T"]), s)
+        _lib.call("fdtd_sg_mse", ptr(b["g"]), ptr(g_target.contiguous()), ng, w_g / ng,
+                  ptr(b["dg"]), ptr(b["loss_g"]), s)
+
     def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8, stream=None):
         self.adam_step += 1
-        _lib.call("fdtd_sg_adam", ptr(self.params), ptr(self.grads), ptr(self.m), ptr(self.v),
-                  self.count, lr, b1, b2, eps, self.adam_step, _s(stream))
-        self._cast(stream)
+        with torch.cuda.device(self.device):
+            _lib.call("fdtd_sg_adam", ptr(self.params), ptr(self.grads), ptr(self.m),
+                      ptr(self.v), self.count, lr, b1, b2, eps, self.adam_step, _s(stream))
+            self._cast(stream)
 
     def train_step(self, density, T_target, g_target, lr=1e-3, w_T=1.0, w_g=1.0, value=False):
         self.forward(density)
