@@ -143,7 +143,10 @@ def reference_case(case, reps=2, checkpoint_every=256):
 def config3(reps=1, workdir=None, pixels=16, h=1e-3, checkpoint_every=256):
     from . import scene
 
-    workdir = Path(workdir or tempfile.mkdtemp(prefix="wfb_config3_"))
+    if workdir is None:
+        with tempfile.TemporaryDirectory(prefix="wfb_config3_") as tmp:
+            return config3(reps, tmp, pixels, h, checkpoint_every)
+    workdir = Path(workdir)
     case = scene.bend_case(workdir / "bend20", steps=4000)
     box = (145, 54, 67, 125, 125, 11)
     material_kwargs = dict(beta=8.0, eps_lo=2.085, contrast=12.11 - 2.085, radius=9, sigma=3.0)
