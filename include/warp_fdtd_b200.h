@@ -104,8 +104,9 @@ int fdtd_gather(float *q, const float *d, const float *hist, void *grad, int gra
  * state, neighbours at +1.  The CPML state ping-pongs: psi0 is read and psi1
  * written when step[0] is even, the other way round when odd (step is the
  * reverse step counter, decremented once per reverse step); both start at
- * zero.  coeff is the (3, clen, 3) table, clen >= max(nx, ny, nz); nx <=
- * 65535 and ny * nz < 2^31. */
+ * zero.  coeff is the CPML table padded to (3, clen, 4) floats (a, b,
+ * 1/kappa, unused), 16-byte aligned, clen >= max(nx, ny, nz); nx <= 65535
+ * and ny * nz < 2^31. */
 int fdtd_reverse_half(int from_h, float *q_dst, const float *q_src, const float *eps,
                       float *psi0, float *psi1, const float *coeff, int clen, const int *step,
                       const float *hist, double *grad, const int *hist_step, int nx, int ny,

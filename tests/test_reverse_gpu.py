@@ -42,6 +42,7 @@ def test_reverse_halves_match_prepare_gather_bitwise():
     step = torch.zeros(1, dtype=torch.int32, device="cuda")
     hstep = torch.zeros(1, dtype=torch.int32, device="cuda")
     s = torch.cuda.current_stream().cuda_stream
+    coeff4 = {f: torch.nn.functional.pad(c, (0, 1)).contiguous() for f, c in coeff.items()}
     for t in (4, 3, 2, 1):  # reverse steps: even, odd, even, odd
         step.fill_(t)
         hstep.fill_(t % 4)
@@ -51,10 +52,10 @@ def test_reverse_halves_match_prepare_gather_bitwise():
         k.gather(qh, d, hist, grad, hstep, nx, ny, nz, *box, 0)
         # step parity 0 reads slot 0 of each pair
         _lib.call("fdtd_reverse_half", 1, ptr(fqe), ptr(fqh), ptr(eps), ptr(ph[0]), ptr(ph[1]),
-                  ptr(coeff["H"]), coeff["H"].shape[1], ptr(step), ptr(hist), ptr(fgrad),
+                  ptr(coeff4["H"]), coeff["H"].shape[1], ptr(step), ptr(hist), ptr(fgrad),
                   ptr(hstep), nx, ny, nz, float(courant), *box, s)
         _lib.call("fdtd_reverse_half", 0, ptr(fqh), ptr(fqe), ptr(eps), ptr(pe[0]), ptr(pe[1]),
-                  ptr(coeff["E"]), coeff["E"].shape[1], ptr(step), None, None, None, nx, ny, nz,
+                  ptr(coeff4["E"]), coeff["E"].shape[1], ptr(step), None, None, None, nx, ny, nz,
                   float(courant), 0, 0, 0, 0, 0, 0, s)
         torch.cuda.synchronize()
         assert torch.equal(fqe, qe) and torch.equal(fqh, qh)

@@ -89,6 +89,9 @@ class Adjoint(Solver):
         self.hist_step = torch.zeros(1, dtype=torch.int32, device=dev)
         self._coeff3 = {f: torch.from_numpy(cpml_coefficients(self.meta, self.data, self.shape, f)).to(dev)
                         for f in "EH"}
+        # the fused halves read (a, b, 1/kappa, 0) as one float4
+        self._coeff4 = {f: torch.nn.functional.pad(c, (0, 1)).contiguous()
+                        for f, c in self._coeff3.items()}
         self.adjoint_sources = []
         self.reverse_graphs = {}
         self.recompute_graphs = {}
@@ -223,13 +226,13 @@ class Adjoint(Solver):
         self.inject(0)
         if self.fused_reverse:
             stream = _lib.stream_handle(self.device)
-            clen = int(self._coeff3["H"].shape[1])
+            clen = int(self._coeff4["H"].shape[1])
             _lib.call("fdtd_reverse_half", 1, ptr(self.qe), ptr(self.qh), ptr(self.eps),
-                      ptr(self.psih), ptr(self.psih2), ptr(self._coeff3["H"]), clen,
+                      ptr(self.psih), ptr(self.psih2), ptr(self._coeff4["H"]), clen,
                       ptr(self.reverse_step), ptr(self.history), ptr(self.grad),
                       ptr(self.hist_step), *self.shape, self.courant, *self.box, stream)
             _lib.call("fdtd_reverse_half", 0, ptr(self.qh), ptr(self.qe), ptr(self.eps),
-                      ptr(self.psie), ptr(self.psie2), ptr(self._coeff3["E"]), clen,
+                      ptr(self.psie), ptr(self.psie2), ptr(self._coeff4["E"]), clen,
                       ptr(self.reverse_step), None, None, None, *self.shape, self.courant,
                       0, 0, 0, 0, 0, 0, stream)
             self.inject(1)

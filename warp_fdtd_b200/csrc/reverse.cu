@@ -20,27 +20,28 @@ namespace wfb {
 // v = factor * q with factor = courant * eps[c] (electric) or -courant;
 // q1 = -v[a], q2 = v[b], a = axis+1, b = axis+2 (mod 3); d = k * q (+ CPML).
 // With psi_out the updated psi of c is written (the cell's own update).
+// co = (a, b, 1/kappa, unused): one 16-byte load per pair.
 template <bool ELECTRIC>
 __device__ __forceinline__ void d_pair(const float *__restrict__ q,
                                        const float *__restrict__ eps,
                                        const float *__restrict__ psi_in, float *psi_out,
-                                       const float *__restrict__ coeff, int clen, i64 n, i64 c,
+                                       const float4 *__restrict__ coeff, int clen, i64 n, i64 c,
                                        int pos, int axis, float courant, float &d1, float &d2) {
     const float factor = ELECTRIC ? courant * eps[c] : -courant;
     const int a = (axis + 1) % 3, b = (axis + 2) % 3;
     const float q1 = -(factor * q[(i64)a * n + c]);
     const float q2 = factor * q[(i64)b * n + c];
-    const float *co = coeff + ((i64)axis * clen + pos) * 3;
-    d1 = co[2] * q1;
-    d2 = co[2] * q2;
-    if (co[0] != 0.0f) {
+    const float4 co = coeff[axis * clen + pos];
+    d1 = co.z * q1;
+    d2 = co.z * q2;
+    if (co.x != 0.0f) {
         const float p1 = psi_in[(i64)(2 * axis) * n + c] + q1;
         const float p2 = psi_in[(i64)(2 * axis + 1) * n + c] + q2;
-        d1 = d1 + co[0] * p1;
-        d2 = d2 + co[0] * p2;
+        d1 = d1 + co.x * p1;
+        d2 = d2 + co.x * p2;
         if (psi_out) {
-            psi_out[(i64)(2 * axis) * n + c] = co[1] * p1;
-            psi_out[(i64)(2 * axis + 1) * n + c] = co[1] * p2;
+            psi_out[(i64)(2 * axis) * n + c] = co.y * p1;
+            psi_out[(i64)(2 * axis + 1) * n + c] = co.y * p2;
         }
     }
 }
@@ -53,7 +54,7 @@ __device__ __forceinline__ void d_pair(const float *__restrict__ q,
 template <bool FROM_H>
 __global__ void reverse_half_kernel(float *__restrict__ q_dst, const float *__restrict__ q_src,
                                     const float *__restrict__ eps, float *psi0, float *psi1,
-                                    const float *__restrict__ coeff, int clen,
+                                    const float4 *__restrict__ coeff, int clen,
                                     const int *__restrict__ step, const float *__restrict__ hist,
                                     double *__restrict__ grad,
                                     const int *__restrict__ hist_step, int nx, int ny, int nz,
@@ -124,6 +125,7 @@ extern "C" int fdtd_reverse_half(int from_h, float *q_dst, const float *q_src, c
                                  int x0, int y0, int z0, int sx, int sy, int sz, void *stream) {
     const i64 n = (i64)nx * ny * nz;
     if (n <= 0 || !q_dst || !q_src || !psi0 || !psi1 || !coeff || !step || psi0 == psi1 ||
+        ((uintptr_t)coeff & 15) ||
         clen < (nx > ny ? (nx > nz ? nx : nz) : (ny > nz ? ny : nz)) || (!from_h && !eps) ||
         (from_h && grad && (!hist || !hist_step || sx < 1 || sy < 1 || sz < 1 || x0 < 0 ||
                             y0 < 0 || z0 < 0 || x0 + sx > nx || y0 + sy > ny || z0 + sz > nz))) {
@@ -137,12 +139,12 @@ extern "C" int fdtd_reverse_half(int from_h, float *q_dst, const float *q_src, c
     const dim3 blocks((unsigned)(((i64)ny * nz + 255) / 256), (unsigned)nx);
     cudaStream_t s = (cudaStream_t)stream;
     if (from_h)
-        reverse_half_kernel<true><<<blocks, 256, 0, s>>>(q_dst, q_src, eps, psi0, psi1, coeff,
-                                                         clen, step, hist, grad, hist_step, nx,
+        reverse_half_kernel<true><<<blocks, 256, 0, s>>>(q_dst, q_src, eps, psi0, psi1,
+                                                         (const float4 *)coeff, clen, step, hist, grad, hist_step, nx,
                                                          ny, nz, courant, x0, y0, z0, sx, sy, sz);
     else
-        reverse_half_kernel<false><<<blocks, 256, 0, s>>>(q_dst, q_src, eps, psi0, psi1, coeff,
-                                                          clen, step, nullptr, nullptr, nullptr,
+        reverse_half_kernel<false><<<blocks, 256, 0, s>>>(q_dst, q_src, eps, psi0, psi1,
+                                                          (const float4 *)coeff, clen, step, nullptr, nullptr, nullptr,
                                                           nx, ny, nz, courant, 0, 0, 0, 0, 0, 0);
     return launch_status("fdtd_reverse_half");
 }
