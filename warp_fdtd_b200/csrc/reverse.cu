@@ -52,7 +52,7 @@ __device__ __forceinline__ void d_pair(const float *__restrict__ q,
 // the updated qE, electric scaling, psi = the E state, neighbours at +1,
 // differences negated.
 template <bool FROM_H>
-__global__ void reverse_half_kernel(float *__restrict__ q_dst, const float *__restrict__ q_src,
+__global__ void __launch_bounds__(256, 8) reverse_half_kernel(float *__restrict__ q_dst, const float *__restrict__ q_src,
                                     const float *__restrict__ eps, float *psi0, float *psi1,
                                     const float4 *__restrict__ coeff, int clen,
                                     const int *__restrict__ step, const float *__restrict__ hist,
@@ -78,18 +78,21 @@ __global__ void reverse_half_kernel(float *__restrict__ q_dst, const float *__re
     d_pair<ELECTRIC>(q_src, eps, psi_in, psi_out, coeff, clen, n, i, x, 0, courant, d[0], d[1]);
     d_pair<ELECTRIC>(q_src, eps, psi_in, psi_out, coeff, clen, n, i, y, 1, courant, d[2], d[3]);
     d_pair<ELECTRIC>(q_src, eps, psi_in, psi_out, coeff, clen, n, i, z, 2, courant, d[4], d[5]);
-    // neighbour pairs (adjoint.py:91-104 `read`: zero outside the grid)
-    float nx0 = 0.0f, nx1 = 0.0f, ny2 = 0.0f, ny3 = 0.0f, nz4 = 0.0f, nz5 = 0.0f;
+    // neighbour pairs (adjoint.py:91-104 `read`: zero outside the grid).  The
+    // pairs are evaluated unconditionally at a clamped neighbour (so every
+    // load can issue early) and replaced by exactly zero outside the grid.
+    float nx0, nx1, ny2, ny3, nz4, nz5;
     const int xn = x + delta, yn = y + delta, zn = z + delta;
-    if (xn >= 0 && xn < nx)
-        d_pair<ELECTRIC>(q_src, eps, psi_in, nullptr, coeff, clen, n, i + (i64)delta * ny * nz,
-                         xn, 0, courant, nx0, nx1);
-    if (yn >= 0 && yn < ny)
-        d_pair<ELECTRIC>(q_src, eps, psi_in, nullptr, coeff, clen, n, i + (i64)delta * nz, yn, 1,
-                         courant, ny2, ny3);
-    if (zn >= 0 && zn < nz)
-        d_pair<ELECTRIC>(q_src, eps, psi_in, nullptr, coeff, clen, n, i + delta, zn, 2, courant,
-                         nz4, nz5);
+    const bool xin = xn >= 0 && xn < nx, yin = yn >= 0 && yn < ny, zin = zn >= 0 && zn < nz;
+    d_pair<ELECTRIC>(q_src, eps, psi_in, nullptr, coeff, clen, n,
+                     xin ? i + (i64)delta * ny * nz : i, xin ? xn : x, 0, courant, nx0, nx1);
+    d_pair<ELECTRIC>(q_src, eps, psi_in, nullptr, coeff, clen, n, yin ? i + (i64)delta * nz : i,
+                     yin ? yn : y, 1, courant, ny2, ny3);
+    d_pair<ELECTRIC>(q_src, eps, psi_in, nullptr, coeff, clen, n, zin ? i + delta : i,
+                     zin ? zn : z, 2, courant, nz4, nz5);
+    if (!xin) nx0 = nx1 = 0.0f;
+    if (!yin) ny2 = ny3 = 0.0f;
+    if (!zin) nz4 = nz5 = 0.0f;
     // gather (adjoint.py:118-150), same operand order
     float v[3];
     v[0] = (ny2 - d[2]) + (nz5 - d[5]);
