@@ -82,10 +82,21 @@ def _timed(adj, reps):
     return out
 
 
-def reference_case(case, reps=2, checkpoint_every=256):
+def _tune(adj):
+    """Time the fused step's launch shapes on this grid (before any graph is
+    captured) and keep the fastest; returns {shape: ms}."""
+    try:
+        timings = adj.autotune(tiles=[2, 3, 4, 5, 6, 8, 10, 12, 14, 16])
+    except ValueError as exc:  # not the full-z path: keep the defaults
+        return {"skipped": str(exc)}
+    return {f"tile {k[0]}, stages {k[1]}, weights {k[2]}": v for k, v in timings.items()}
+
+
+def reference_case(case, reps=2, checkpoint_every=256, tune=False):
     case = Path(case)
     adj = Adjoint(case, checkpoint_every=checkpoint_every)
     attach(adj)
+    tuned = _tune(adj) if tune else None
     p0 = np.asarray(adj.data["parameters/p0"])[..., 0]
     x0, y0, z0, sx, sy, sz = adj.box
     beta = adj.meta.get("beta", 50.0)
@@ -94,7 +105,8 @@ def reference_case(case, reps=2, checkpoint_every=256):
     reference = np.asarray(adj.data["inv_permittivity"])[0, x0:x0 + sx, y0:y0 + sy, z0]
     res = dict(case=str(case), shape=list(adj.shape), time_steps=adj.steps,
                box=list(adj.box), material_max_absolute_error=float(
-                   np.max(np.abs(projected - reference))))
+                   np.max(np.abs(projected - reference))),
+               launch_shape=dict(tile_y=adj.tile[0], stages=adj.stages, autotune=tuned))
     loss, grad = adj.differentiate(p0)  # builds the graphs
     times = _timed(adj, reps)
     res.update(seconds=[t[0] for t in times], forward_seconds=[t[1] for t in times],
@@ -140,12 +152,12 @@ def reference_case(case, reps=2, checkpoint_every=256):
     return res
 
 
-def config3(reps=1, workdir=None, pixels=16, h=1e-3, checkpoint_every=256):
+def config3(reps=1, workdir=None, pixels=16, h=1e-3, checkpoint_every=256, tune=False):
     from . import scene
 
     if workdir is None:
         with tempfile.TemporaryDirectory(prefix="wfb_config3_") as tmp:
-            return config3(reps, tmp, pixels, h, checkpoint_every)
+            return config3(reps, tmp, pixels, h, checkpoint_every, tune)
     workdir = Path(workdir)
     case = scene.bend_case(workdir / "bend20", steps=4000)
     box = (145, 54, 67, 125, 125, 11)
@@ -153,6 +165,7 @@ def config3(reps=1, workdir=None, pixels=16, h=1e-3, checkpoint_every=256):
     adj = Adjoint(case, box=box, checkpoint_every=checkpoint_every,
                   material_kwargs=material_kwargs)
     attach(adj)
+    tuned = _tune(adj) if tune else None
     p = np.random.default_rng(0).uniform(0, 1, (125, 125)).astype(np.float32)
     loss, grad = adj.differentiate(p)
     times = _timed(adj, reps)
@@ -162,7 +175,8 @@ def config3(reps=1, workdir=None, pixels=16, h=1e-3, checkpoint_every=256):
                backward_seconds=[t[2] for t in times],
                cell_updates=int(np.prod(adj.shape)) * adj.steps,
                history_bytes=int(adj.history.numel() * 4),
-               checkpoint_every=adj.checkpoint_every)
+               checkpoint_every=adj.checkpoint_every,
+               launch_shape=dict(tile_y=adj.tile[0], stages=adj.stages, autotune=tuned))
     g = np.asarray(grad, np.float64).ravel()
     rng = np.random.default_rng(16)
     top = np.flatnonzero(np.abs(g) >= np.quantile(np.abs(g), 0.75))
@@ -192,12 +206,14 @@ def main(argv=None):
     ap.add_argument("--checkpoint-every", type=int, default=256,
                     help="steps per checkpoint segment; >= the step count keeps the whole "
                          "design-box history and skips the recomputation")
+    ap.add_argument("--autotune", action="store_true",
+                    help="time the fused step's launch shapes on the grid first")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     if a.reps < 1:
         ap.error("--reps must be positive")
-    res = (config3(reps=a.reps, checkpoint_every=a.checkpoint_every) if a.config3
-           else reference_case(a.case, a.reps, a.checkpoint_every))
+    res = (config3(reps=a.reps, checkpoint_every=a.checkpoint_every, tune=a.autotune)
+           if a.config3 else reference_case(a.case, a.reps, a.checkpoint_every, a.autotune))
     text = json.dumps(res, indent=2)
     if a.out:
         Path(a.out).write_text(text + "\n")
