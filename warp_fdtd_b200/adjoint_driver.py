@@ -114,10 +114,13 @@ class Adjoint(Solver):
                       y0, z0, sx, sy, sz, float(self.courant), stream)
             _lib.call("fdtd_advance", ptr(self.hist_step), 1, stream)
 
-    def run(self):
+    def run(self, sync=True):
         """Forward trajectory with detectors, saving a state checkpoint every
         `checkpoint_every` steps (at step counts that are multiples of it);
-        with a single segment the design-box history is recorded instead."""
+        with a single segment the design-box history is recorded instead.
+        Everything is enqueued on the current stream; sync=False returns
+        without waiting for the device (batch.BatchAdjoint overlaps
+        instances that way)."""
         K = self.checkpoint_every
         self.checkpoints = {}
         self._history_fresh = False
@@ -145,7 +148,8 @@ class Adjoint(Solver):
                         self.checkpoints[self._issued] = self._snapshot()
                     self.launch_step()
             self._history_fresh = self.history_in_forward
-            torch.cuda.synchronize(self.device)
+            if sync:
+                torch.cuda.synchronize(self.device)
 
     def _recompute_step(self, stream):
         _lib.call("fdtd_step_fused", self._args, stream)
@@ -280,8 +284,9 @@ class Adjoint(Solver):
                 self.recompute_graphs[length] = g
         self.reset_reverse()
 
-    def backward(self):
-        """Reverse sweep over all segments, last first."""
+    def backward(self, sync=True):
+        """Reverse sweep over all segments, last first, enqueued on the current
+        stream (sync=False: no wait for the device at the end)."""
         with torch.cuda.device(self.device):
             for start, length in reversed(self._segments()):
                 if not (self._history_fresh and start == 0 and length == self.steps):
@@ -295,7 +300,8 @@ class Adjoint(Solver):
                 else:
                     g.replay()
             self._history_fresh = False
-            torch.cuda.synchronize(self.device)
+            if sync:
+                torch.cuda.synchronize(self.device)
 
     # ------------------------------------------------------------ design
     def set_design(self, parameters):
