@@ -83,3 +83,48 @@ def test_new_entry_points_reject_bad_arguments(lib):
     blocks, sms = ctypes.c_int(), ctypes.c_int()
     assert L.fdtd_step_occupancy(ctypes.byref(a), ctypes.byref(blocks), ctypes.byref(sms)) == -1
     assert b"full-z" in L.fdtd_last_error()
+
+
+def test_surrogate_and_reverse_entry_points_reject_bad_arguments(lib):
+    """The surrogate's GEMM and layer kernels and the fused reverse halves
+    check their arguments on the host, before any launch."""
+    from warp_fdtd_b200 import _lib
+
+    L = _lib.load()
+    g = _lib.SgGemmArgs()
+    assert L.fdtd_sg_gemm(ctypes.byref(g), None) == -1  # null operands
+    g.A, g.B, g.C = 16, 32, 48
+    g.M, g.N, g.K, g.lda, g.ldb, g.ldc = 128, 32, 64, 64, 64, 32
+    g.lda = 60  # not a multiple of 8
+    assert L.fdtd_sg_gemm(ctypes.byref(g), None) == -1
+    g.lda, g.A = 64, 17  # misaligned A
+    assert L.fdtd_sg_gemm(ctypes.byref(g), None) == -1
+    g.A, g.K, g.lda, g.ldb = 16, 1000, 1000, 1000
+    g.splits, g.relu = 4, 1  # split K (16 chunks of 64) with an epilogue
+    assert L.fdtd_sg_gemm(ctypes.byref(g), None) == -1
+    g.relu, g.splits, g.layout = 0, 1, 2  # unknown operand layout
+    assert L.fdtd_sg_gemm(ctypes.byref(g), None) == -1
+    assert b"layout" in L.fdtd_last_error()
+    g.splits = 37  # more than the 16 chunks of 64
+    assert L.fdtd_sg_gemm_splits(ctypes.byref(g)) == 16
+    g.splits = 5
+    assert L.fdtd_sg_gemm_splits(ctypes.byref(g)) == 4  # 4 chunks each
+    assert L.fdtd_sg_im2col(None, 1, 1, 4, 4, 1, None, 16, None) == -1
+    assert L.fdtd_sg_im2col(16, 1, 1, 4, 4, 1, 32, 8, None) == -1  # ldcol < 9 C
+    assert L.fdtd_sg_pool(16, 8, 1, 5, 4, 8, 32, 8, None) == -1  # odd H
+    assert L.fdtd_sg_transpose(16, 4, 8, 8, 32, 4, None) == -1  # lds < cols
+    assert L.fdtd_sg_splitk_reduce(16, 2, 10, 4, 4, 4, 32, 4, 0, None) == -1  # stride
+    assert L.fdtd_sg_adam(16, 16, 16, 16, 10, 1e-3, 0.9, 0.999, 1e-8, 0, None) == -1
+    # fused reverse halves
+    assert L.fdtd_reverse_half(1, None, None, None, None, None, None, 8, None, None, None,
+                               None, 4, 4, 4, 0.5, 0, 0, 0, 0, 0, 0, None) == -1
+    assert L.fdtd_reverse_half(0, 16, 32, 48, 64, 64, 96, 8, 112, None, None, None, 4, 4, 4,
+                               0.5, 0, 0, 0, 0, 0, 0, None) == -1  # psi0 == psi1
+    assert L.fdtd_reverse_half(0, 16, 32, 48, 64, 80, 100, 8, 112, None, None, None, 4, 4, 4,
+                               0.5, 0, 0, 0, 0, 0, 0, None) == -1  # misaligned table
+    assert L.fdtd_reverse_half(0, 16, 32, 48, 64, 80, 96, 3, 112, None, None, None, 4, 4, 4,
+                               0.5, 0, 0, 0, 0, 0, 0, None) == -1  # clen < max dim
+    assert L.fdtd_reverse_half(0, 16, 32, None, 64, 80, 96, 8, 112, None, None, None, 4, 4, 4,
+                               0.5, 0, 0, 0, 0, 0, 0, None) == -1  # electric half needs eps
+    assert L.fdtd_reverse_half(1, 16, 32, 48, 64, 80, 96, 8, 112, 128, 144, 160, 4, 4, 4, 0.5,
+                               2, 0, 0, 4, 4, 4, None) == -1  # design box outside the grid
