@@ -134,7 +134,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(backend="nccl"):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE): each
+    rank binds its own GPU; with world > 1 a process group of `backend`
+    (nccl on GPUs, gloo for the host-only tests) carries the timing
+    reductions, never field data (replicas)."""
     import torch
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -144,10 +148,13 @@ def dist_setup():
         import datetime
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-    else:
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
+    elif backend == "nccl":
         torch.cuda.set_device(0)
     return world, rank, local
 
@@ -159,26 +166,30 @@ def barrier(world):
         dist.barrier()
 
 
-def reduce_max(value, world):
+def _reduce(value, world, op):
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def reduce_max(value, world):
+    """Max over ranks (the job's time is its slowest rank's)."""
+    import torch.distributed as dist
+
+    return _reduce(value, world, dist.ReduceOp.MAX) if world > 1 else value
 
 
 def reduce_sum(value, world):
-    if world == 1:
-        return value
-    import torch
+    """Sum over ranks (the job's cell-updates)."""
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(value, world, dist.ReduceOp.SUM) if world > 1 else value
 
 
 def cpu_sample(case, time_steps, threads=None):
