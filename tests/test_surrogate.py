@@ -77,3 +77,39 @@ def test_parameter_count_of_default_network():
     p = osg.init_params(base=32, nwav=8)
     n = sum(v.size for v in p.values())
     assert 1.0e6 < n < 1.3e6, n
+
+
+def test_conv_as_gemm_equals_direct_correlation():
+    """im2col(x) . W^T with W[cout, tap*C + c] is the 3 x 3 'same' correlation
+    out[p, o] = sum over (dy, dx, c) of x[y+dy, x+dx, c] * W[o, ((dy+1)*3 + dx+1)*C + c]."""
+    rng = np.random.default_rng(3)
+    B, H, W, C, O = 2, 5, 7, 3, 4
+    x = rng.standard_normal((B * H * W, C))
+    w = rng.standard_normal((O, 9 * C))
+    got = osg.im2col(x, H, W) @ w.T
+    xi = x.reshape(B, H, W, C)
+    want = np.zeros((B, H, W, O))
+    for b in range(B):
+        for yy in range(H):
+            for xx in range(W):
+                for dy in (-1, 0, 1):
+                    for dx in (-1, 0, 1):
+                        sy, sx = yy + dy, xx + dx
+                        if 0 <= sy < H and 0 <= sx < W:
+                            tap = (dy + 1) * 3 + (dx + 1)
+                            want[b, yy, xx] += w[:, tap * C:(tap + 1) * C] @ xi[b, sy, sx]
+    np.testing.assert_allclose(got.reshape(B, H, W, O), want, rtol=1e-12, atol=1e-12)
+
+
+def test_bf16_network_tracks_the_exact_network():
+    """The bf16-rounded forward stays within bf16 accuracy of the float64 one."""
+    p = osg.init_params(seed=5, base=8, nwav=4)
+    rng = np.random.default_rng(6)
+    for k in p:
+        if k.endswith(".b"):
+            p[k] = rng.uniform(0.0, 0.05, p[k].shape).astype(np.float32)
+    x = rng.uniform(0, 1, (2, 16, 16))
+    T16, g16 = osg.OracleSurrogate(p, (16, 16), 4, 8, bf16=True).forward(x.astype(np.float32))
+    T64, g64 = osg.OracleSurrogate(p, (16, 16), 4, 8, bf16=False, dtype=np.float64).forward(x)
+    assert np.linalg.norm(T16 - T64) / np.linalg.norm(T64) < 3e-2
+    assert np.linalg.norm(g16 - g64) / np.linalg.norm(g64) < 3e-2
