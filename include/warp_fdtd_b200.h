@@ -120,6 +120,19 @@ int fdtd_inject(float *qe, float *qh, const float *source, const float *weights,
                 const int *step, int nx, int ny, int nz, int x0, int y0, int z0, int sx,
                 int sy, int sz, int old_h_only, void *stream);
 
+/* fdtd_inject for up to FDTD_INJECT_PLANES_MAX planes in one launch (the
+ * adjoint's mode planes of one half step), each with its own source
+ * (6, sx*sy*sz, 2), weights (steps, 2) and extent.  The same scattered sums;
+ * float32 atomics, so the summation order differs from separate launches. */
+#define FDTD_INJECT_PLANES_MAX 8
+typedef struct fdtd_inject_plane {
+    const float *source;
+    const float *weights;
+    int x0, y0, z0, sx, sy, sz;
+} fdtd_inject_plane;
+int fdtd_inject_many(float *qe, float *qh, const fdtd_inject_plane *planes, int nplanes,
+                     const int *step, int nx, int ny, int nz, int old_h_only, void *stream);
+
 /* Replaces adjoint.py:472-490 `write_design`: eps[box] = plane[x, y] for all z
  * in the box; plane is (sx, sy) float32. */
 int fdtd_write_design(const float *plane, float *eps, int nx, int ny, int nz, int x0,

@@ -82,6 +82,13 @@ class BatchPlan(ctypes.Structure):
                                         "stages", "vector", "full_rows", "base", "device")]
 
 
+class InjectPlane(ctypes.Structure):
+    """Mirror of `fdtd_inject_plane`."""
+
+    _fields_ = [("source", _p), ("weights", _p)] + [
+        (name, _i) for name in ("x0", "y0", "z0", "sx", "sy", "sz")]
+
+
 class SgGemmArgs(ctypes.Structure):
     """Mirror of `fdtd_sg_gemm_args`."""
 
@@ -125,6 +132,7 @@ _SIGNATURES = {
     "fdtd_record_stage": [_p, _p, _p, _p, _p, _p, _i, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i,
                           _i, _i, _i, _p],
     "fdtd_dft_fold": [_p, _p, _i, _p, _i, _p, _i, _p, _ll, _p],
+    "fdtd_inject_many": [_p, _p, ctypes.POINTER(InjectPlane), _i, _p, _i, _i, _i, _i, _p],
     "fdtd_reverse_half": [_i, _p, _p, _p, _p, _p, _p, _i, _p, _p, _p, _p, _i, _i, _i, _f, _i,
                           _i, _i, _i, _i, _i, _p],
     "fdtd_sg_gemm": [ctypes.POINTER(SgGemmArgs), _p],

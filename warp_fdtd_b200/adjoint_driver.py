@@ -84,9 +84,13 @@ class Adjoint(Solver):
         self.fused_reverse = bool(fused_reverse)
         self.psie2 = torch.zeros((6, n), **f32) if self.fused_reverse else None
         self.psih2 = torch.zeros((6, n), **f32) if self.fused_reverse else None
+        self._inject_planes = None  # fused path: all planes' injections in one launch
         self.grad = torch.zeros(self.design_n, dtype=torch.float64, device=dev)
         self.reverse_step = torch.zeros(1, dtype=torch.int32, device=dev)
         self.hist_step = torch.zeros(1, dtype=torch.int32, device=dev)
+        # fused path: both counters advanced by one launch
+        self._counters = torch.tensor([self.reverse_step.data_ptr(), self.hist_step.data_ptr()],
+                                      dtype=torch.int64, device=dev)
         self._coeff3 = {f: torch.from_numpy(cpml_coefficients(self.meta, self.data, self.shape, f)).to(dev)
                         for f in "EH"}
         # the fused halves read (a, b, 1/kappa, 0) as one float4
@@ -218,7 +222,27 @@ class Adjoint(Solver):
                 v = host.to(self.device)
             self.adjoint_sources.append((m, v))
 
+    def _planes(self):
+        """The adjoint sources as fdtd_inject_plane entries (their buffers are
+        updated in place by prepare_sources, so the entries stay valid)."""
+        key = tuple((id(m), v.data_ptr()) for m, v in self.adjoint_sources)
+        if self._inject_planes is None or self._inject_planes[0] != key:
+            arr = (_lib.InjectPlane * len(self.adjoint_sources))()
+            for pl, (m, v) in zip(arr, self.adjoint_sources):
+                sy, sz = (int(d) for d in m.shape[1:])
+                pl.source, pl.weights = ptr(v), ptr(m.weights[0])
+                pl.x0, pl.y0, pl.z0 = (int(c) for c in m.lo)
+                pl.sx, pl.sy, pl.sz = int(v.shape[1]) // (sy * sz), sy, sz
+            self._inject_planes = (key, arr)
+        return self._inject_planes[1]
+
     def inject(self, old):
+        if self.fused_reverse and 1 <= len(self.adjoint_sources) <= 8:
+            planes = self._planes()
+            _lib.call("fdtd_inject_many", ptr(self.qe), ptr(self.qh), planes, len(planes),
+                      ptr(self.reverse_step), *self.shape, int(old),
+                      _lib.stream_handle(self.device))
+            return
         for m, v in self.adjoint_sources:
             kernels.inject(self.qe, self.qh, v, m.weights[0], self.reverse_step, *self.shape,
                            *m.lo, *m.shape[1:], old)
@@ -240,8 +264,7 @@ class Adjoint(Solver):
                       ptr(self.reverse_step), None, None, None, *self.shape, self.courant,
                       0, 0, 0, 0, 0, 0, stream)
             self.inject(1)
-            _lib.call("fdtd_advance", ptr(self.reverse_step), -1, stream)
-            _lib.call("fdtd_advance", ptr(self.hist_step), -1, stream)
+            _lib.call("fdtd_advance_many", ptr(self._counters), 2, -1, stream)
             return
         common = [*self.shape, self.courant]
         kernels.prepare(self.qh, self.eps, self.psih, self._coeff3["H"], self.d, *common, 0)

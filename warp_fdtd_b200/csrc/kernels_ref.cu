@@ -336,16 +336,15 @@ __device__ __forceinline__ void add_q(float *q, i64 n, int c, int x, int y, int 
     if (inside(x, y, z, nx, ny, nz)) atomicAdd(q + (i64)c * n + flat(x, y, z, ny, nz), value);
 }
 
-// adjoint.py:181-223 `inject`.
-__global__ void inject_kernel(float *__restrict__ qe, float *__restrict__ qh,
-                              const float2 *__restrict__ source,
-                              const float2 *__restrict__ weights,
-                              const int *__restrict__ step, int nx, int ny, int nz, int x0,
-                              int y0, int z0, int sx, int sy, int sz, int old_h_only) {
+// adjoint.py:181-223 `inject` for plane cell i of one plane.
+__device__ __forceinline__ void inject_cell(float *__restrict__ qe, float *__restrict__ qh,
+                                            const float2 *__restrict__ source,
+                                            const float2 *__restrict__ weights,
+                                            const int *__restrict__ step, int nx, int ny,
+                                            int nz, int x0, int y0, int z0, int sx, int sy,
+                                            int sz, int old_h_only, i64 i) {
     const i64 n = (i64)nx * ny * nz;
     const i64 count = (i64)sx * sy * sz;
-    i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
     float2 w = weights[step[0]];
     if (!(fabsf(w.x) + fabsf(w.y) > 0.0f)) return;
     int x = x0 + (int)(i / ((i64)sy * sz));
@@ -370,6 +369,38 @@ __global__ void inject_kernel(float *__restrict__ qe, float *__restrict__ qh,
         for (int dy = 0; dy < 2; ++dy)
             for (int dz = 0; dz < 2; ++dz)
                 add_q(qh, n, 2, x - dx, y - dy, z + dz, nx, ny, nz, 0.0625f * v[5]);
+}
+
+__global__ void inject_kernel(float *__restrict__ qe, float *__restrict__ qh,
+                              const float2 *__restrict__ source,
+                              const float2 *__restrict__ weights,
+                              const int *__restrict__ step, int nx, int ny, int nz, int x0,
+                              int y0, int z0, int sx, int sy, int sz, int old_h_only) {
+    const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (i64)sx * sy * sz) return;
+    inject_cell(qe, qh, source, weights, step, nx, ny, nz, x0, y0, z0, sx, sy, sz, old_h_only,
+                i);
+}
+
+// Several planes' injections in one launch: thread i belongs to the plane
+// whose cell range [start[k], start[k+1]) holds it.
+struct InjectPlanes {
+    fdtd_inject_plane p[FDTD_INJECT_PLANES_MAX];
+    i64 start[FDTD_INJECT_PLANES_MAX + 1];
+    int count;
+};
+
+__global__ void inject_many_kernel(float *__restrict__ qe, float *__restrict__ qh,
+                                   const __grid_constant__ InjectPlanes planes,
+                                   const int *__restrict__ step, int nx, int ny, int nz,
+                                   int old_h_only) {
+    const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= planes.start[planes.count]) return;
+    int k = 0;
+    while (k + 1 < planes.count && i >= planes.start[k + 1]) ++k;
+    const fdtd_inject_plane &pl = planes.p[k];
+    inject_cell(qe, qh, (const float2 *)pl.source, (const float2 *)pl.weights, step, nx, ny, nz,
+                pl.x0, pl.y0, pl.z0, pl.sx, pl.sy, pl.sz, old_h_only, i - planes.start[k]);
 }
 
 // adjoint.py:472-490 `write_design`.
@@ -539,6 +570,31 @@ int fdtd_inject(float *qe, float *qh, const float *source, const float *weights,
         qe, qh, (const float2 *)source, (const float2 *)weights, step, nx, ny, nz, x0, y0, z0,
         sx, sy, sz, old_h_only);
     return launch_status("fdtd_inject");
+}
+
+int fdtd_inject_many(float *qe, float *qh, const fdtd_inject_plane *planes, int nplanes,
+                     const int *step, int nx, int ny, int nz, int old_h_only, void *stream) {
+    if (!qe || !qh || !planes || !step || nplanes < 1 || nplanes > FDTD_INJECT_PLANES_MAX ||
+        nx < 1 || ny < 1 || nz < 1) {
+        set_error("fdtd_inject_many: invalid arguments (1 to %d planes)",
+                  FDTD_INJECT_PLANES_MAX);
+        return FDTD_ERR_ARG;
+    }
+    InjectPlanes pp;
+    pp.count = nplanes;
+    pp.start[0] = 0;
+    for (int k = 0; k < nplanes; ++k) {
+        const fdtd_inject_plane &pl = planes[k];
+        if (!pl.source || !pl.weights || pl.sx < 1 || pl.sy < 1 || pl.sz < 1) {
+            set_error("fdtd_inject_many: plane %d has no source, weights or cells", k);
+            return FDTD_ERR_ARG;
+        }
+        pp.p[k] = pl;
+        pp.start[k + 1] = pp.start[k] + (i64)pl.sx * pl.sy * pl.sz;
+    }
+    inject_many_kernel<<<blocks_for(pp.start[nplanes], 256), 256, 0, as_stream(stream)>>>(
+        qe, qh, pp, step, nx, ny, nz, old_h_only);
+    return launch_status("fdtd_inject_many");
 }
 
 int fdtd_write_design(const float *plane, float *eps, int nx, int ny, int nz, int x0,
