@@ -119,7 +119,10 @@ def adjoint_loop(problem, p0, target=0.9, iters=100, step=0.1, record=None):
 
 
 class Dataset:
-    """Device-resident (density, spectrum, normalised gradient) triples."""
+    """(density, spectrum, gradient) triples kept on the host; tensors()
+    uploads them with the gradients divided by g_scale, the RMS gradient of
+    the data present at the first call (or the value given), kept fixed so
+    later additions are scaled alike."""
 
     def __init__(self, shape, nwav, device="cuda:0", g_scale=None):
         self.shape, self.nwav, self.device = shape, nwav, torch.device(device)
