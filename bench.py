@@ -24,6 +24,7 @@ on a bounded sample of the same workload per step.
 """
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -316,24 +317,38 @@ def run_ours(args, world, rank, local):
     # monitor's folds (every `batch` steps and at the end)
     planes, grouped = s._staged_planes()
     own = sum(1 for m in s.monitors if m.shared is None and id(m) not in grouped)
-    launches_per_step = 1 + own + 1  # the grouped recorder also advances the counter
+    recorders_per_step = own + 1  # the grouped recorder also advances the counter
+    pairs, singles = s.step_launches()
     folds = sum(-(-s.steps // m.batch) for m in s.monitors if m.is_phasor and m.shared is None)
 
-    # dominant kernel alone: average duration of the fused step over 200 launches
+    # dominant kernel alone: average duration of the step kernel the
+    # trajectory runs (two time steps per launch at time_block 2) over 200
+    # launches on the launching stream
     s.reset()
+    kernel_name, updates = "fz_step_kernel (fdtd_step_fused, one step)", 1
+    launch = lambda: _lib.call("fdtd_step_fused", s._args, stream.cuda_stream)
+    if s.time_block == 2:
+        info, extra = s._block[2], s._pair_extra()
+        kernel_name, updates = "block_step_kernel (fdtd_step_block, two steps per launch)", 2
+        launch = lambda: _lib.call("fdtd_step_block", ctypes.byref(info["args"][s._rel]),
+                                   ctypes.byref(info["plan"]), ctypes.byref(extra),
+                                   stream.cuda_stream)
+    elif s.time_block == 1:
+        kernel_name = "block_step_kernel (fdtd_step_block, one step per launch)"
+        launch = lambda: s._step_kernel(stream.cuda_stream)
     for _ in range(5):
-        _lib.call("fdtd_step_fused", s._args, stream.cuda_stream)
+        launch()
     k0 = torch.cuda.Event(enable_timing=True)
     k1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     k0.record(stream)
     nk = 200
     for _ in range(nk):
-        _lib.call("fdtd_step_fused", s._args, stream.cuda_stream)
+        launch()
     k1.record(stream)
     torch.cuda.synchronize()
     kernel_ms = k0.elapsed_time(k1) / nk
-    achieved = BYTES_PER_CELL * s.n / (kernel_ms / 1e3) / 1e9
+    achieved = BYTES_PER_CELL * s.n * updates / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = load_peaks()
     traffic = None
     tfile = ROOT / "profiles" / "fused_step_traffic.json"
@@ -388,14 +403,15 @@ def run_ours(args, world, rank, local):
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "fz_step_kernel (fdtd_step_fused, path 3)",
+                         "kernel": kernel_name, "cell_updates_per_launch": updates,
                          "kernel_ms": kernel_ms, "bytes_per_cell": BYTES_PER_CELL,
                          "peak_kind": f"{peak_kind} (copy bandwidth)"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "Gcell-updates/s",
                     "h2d_bytes_per_step": int(host_mat.numel()),
                     "d2h_bytes_per_step": int(phasor_bytes)},
-            "gpu_launches": int((launches_per_step * s.steps + folds) * args.steps),
+            "gpu_launches": int((pairs + singles + recorders_per_step * s.steps + folds)
+                                * args.steps),
             "clocks": clock_info,
             "modal_transmission_1550nm": meas.get("modal_transmission_spectrum", [None] * 3)[2],
             "surrogate_train": surrogate,

@@ -306,6 +306,57 @@ int fdtd_advance_many(int *const *steps, int count, int delta, void *stream);
 /* Free a prepared batch's parameter slots (the workspace is the caller's). */
 int fdtd_batch_release(fdtd_batch_plan *plan);
 
+/* Time-blocked fused step: one launch advances E and H by `depth` (1 or 2)
+ * time steps, the work of depth x solver.py:194-237's update_e + update_h
+ * launches (kernels.py:77-148), reading every plane of E(n), H(n-1/2) once
+ * and writing E(n+depth), H(n+depth-1/2) once.  Arguments and buffer
+ * convention as fdtd_step_fused with the slab CPML layout (path 3): with t =
+ * step[0] and s = t & 1 it reads E[s], H[s], psi_*[s] and writes E[s^1],
+ * H[s^1], psi_*[s^1] (the depth-step result), and does not advance step[0].
+ * Bitwise equal to `depth` single steps.  No reference counterpart (the
+ * reference launches one sweep per field and step).
+ *
+ * fdtd_step_block_prepare (synchronous: call it outside stream capture)
+ * reads the z CPML coefficients, orders the groups of four z cells so that the
+ * ones carrying z CPML run in warps of their own, picks the tile (args->tile_y
+ * or, when 0, the tallest that fits) and fills *plan.  args->stages (2..4,
+ * default 2) sizes shared memory.  fdtd_step_block launches
+ * args->schedule_blocks blocks, block b running the schedule's int4 entries
+ * (y tile, first plane, end plane, 0) b*segments .. b*segments+segments-1 in
+ * order (extra->segments, default 1; a tile < 0 ends the block's list, and
+ * args->chunk_x must be at least the longest entry), or one block per tile x
+ * chunk_x planes without a schedule.  extra may be NULL at depth 1.
+ * Depth 2 keeps the CPML state between its two steps in `extra->scratch`
+ * (plan->scratch_block_bytes per block, 16-byte aligned, no initial contents)
+ * and can write E(n+1) and H(n+1/2) of the cells inside up to
+ * FDTD_SNAP_BOXES_MAX boxes (x0, x1, y0, y1, z0, z1, half-open; whole groups
+ * of four z cells) to snap_e / snap_h ((3, nx*ny*pitch_z) each), so that
+ * detectors can sample the intermediate step. */
+#define FDTD_BLOCK_GROUPS_MAX 64
+#define FDTD_SNAP_BOXES_MAX 8
+typedef struct fdtd_block_plan {
+    int depth, tile_y, stages, rows, threads;
+    int groups_plain, groups_slab;   /* groups of 4 z cells without / with z CPML */
+    unsigned char group[FDTD_BLOCK_GROUPS_MAX];  /* plain groups, then slab groups */
+    long long scratch_block_bytes;   /* depth 2: scratch bytes per block */
+    int pair_blocks;                 /* 1: two blocks per SM (registers capped) */
+    int device, blocks_per_sm, sms;
+} fdtd_block_plan;
+
+typedef struct fdtd_block_extra {
+    float *scratch;
+    long long scratch_bytes;
+    float *snap_e, *snap_h;
+    int segments;  /* schedule entries per block (default 1): block b runs entries
+                      b*segments .. b*segments+segments-1 in order, tile < 0 ends the list */
+    int nsnap;
+    int snap_box[FDTD_SNAP_BOXES_MAX][6];
+} fdtd_block_extra;
+
+int fdtd_step_block_prepare(const fdtd_step_args *args, int depth, fdtd_block_plan *plan);
+int fdtd_step_block(const fdtd_step_args *args, const fdtd_block_plan *plan,
+                    const fdtd_block_extra *extra, void *stream);
+
 /* Fill the full-z path's launch-shape defaults into *args (tile_y where 0;
  * chunk_x where 0 and no schedule is set), as fdtd_step_fused would pick
  * them.  No reference counterpart. */

@@ -65,7 +65,12 @@ def test_autotune_keeps_the_fastest_shape_and_parity(tmp_path):
     case = make_bundle(tmp_path / "b", (16, 13, 36), 12, seed=4)
     s = Solver(case)
     timings = s.autotune(repeats=3)
-    assert timings and min(timings, key=timings.get) == (s.tile[0], s.stages, s.schedule_weights)
+    # the time-blocked kernel: (depth, tile rows, stages), per-step times
+    best = min(timings, key=timings.get)
+    assert best == (s.time_block, *s.block_shape[s.time_block])
+    s0 = Solver(case, time_block=0)
+    t0 = s0.autotune(repeats=3)
+    assert t0 and min(t0, key=t0.get) == (s0.tile[0], s0.stages, s0.schedule_weights)
     s.reset()
     s.run()
     o = OracleSolver(case)

@@ -82,6 +82,26 @@ class BatchPlan(ctypes.Structure):
                                         "stages", "vector", "full_rows", "base", "device")]
 
 
+BLOCK_GROUPS_MAX = 64
+SNAP_BOXES_MAX = 8
+
+
+class BlockPlan(ctypes.Structure):
+    """Mirror of `fdtd_block_plan`."""
+
+    _fields_ = ([(name, _i) for name in ("depth", "tile_y", "stages", "rows", "threads",
+                                         "groups_plain", "groups_slab")]
+                + [("group", ctypes.c_ubyte * BLOCK_GROUPS_MAX), ("scratch_block_bytes", _ll)]
+                + [(name, _i) for name in ("pair_blocks", "device", "blocks_per_sm", "sms")])
+
+
+class BlockExtra(ctypes.Structure):
+    """Mirror of `fdtd_block_extra`."""
+
+    _fields_ = [("scratch", _p), ("scratch_bytes", _ll), ("snap_e", _p), ("snap_h", _p),
+                ("segments", _i), ("nsnap", _i), ("snap_box", (_i * 6) * SNAP_BOXES_MAX)]
+
+
 class InjectPlane(ctypes.Structure):
     """Mirror of `fdtd_inject_plane`."""
 
@@ -127,6 +147,9 @@ _SIGNATURES = {
     "fdtd_material_forward_noalloc": [_p, _p, _i, _p, _i, _i, _f, _f, _f, _p],
     "fdtd_material_backward": [_p, _p, _i, _p, _p, _p, _i, _i, _f, _f, _f, _p],
     "fdtd_step_fused": [ctypes.POINTER(StepArgs), _p],
+    "fdtd_step_block_prepare": [ctypes.POINTER(StepArgs), _i, ctypes.POINTER(BlockPlan)],
+    "fdtd_step_block": [ctypes.POINTER(StepArgs), ctypes.POINTER(BlockPlan),
+                        ctypes.POINTER(BlockExtra), _p],
     "fdtd_record_phasor64": [_p, _p, _p, _p, _p, _p, _i, _p, _i, _p, _i, _i, _i, _i, _i, _i,
                              _i, _i, _i, _i, _i, _p],
     "fdtd_record_stage": [_p, _p, _p, _p, _p, _p, _i, _p, _i, _i, _i, _i, _i, _i, _i, _i, _i,

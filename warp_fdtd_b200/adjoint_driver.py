@@ -35,7 +35,10 @@ from .solver import Solver, cpml_coefficients
 class Adjoint(Solver):
     def __init__(self, case, box=None, checkpoint_every=256, strict=False, device="cuda:0",
                  graph_steps=64, material_kwargs=None, fused_reverse=True):
-        super().__init__(case, device=device, graph_steps=graph_steps, material="f32")
+        # single steps (the design-box history and the checkpoints need every
+        # step's fields in the parity buffers)
+        super().__init__(case, device=device, graph_steps=graph_steps, material="f32",
+                         time_block=1)
         settings = self.meta["settings"]
         if strict:
             if (
@@ -156,7 +159,7 @@ class Adjoint(Solver):
                 torch.cuda.synchronize(self.device)
 
     def _recompute_step(self, stream):
-        _lib.call("fdtd_step_fused", self._args, stream)
+        self._step_kernel(stream)
         x0, y0, z0, sx, sy, sz = self.box
         _lib.call("fdtd_record_curl_pp", ptr(self._H[0]), ptr(self._H[1]), self._pitch,
                   ptr(self.step), ptr(self.hist_step), ptr(self.history), *self.shape, x0, y0, z0,

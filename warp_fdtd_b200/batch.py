@@ -112,7 +112,7 @@ class BatchSolver:
                   self._blocks, stream)
         for s in self.solvers:
             for m in s.monitors:
-                m.launch(s)
+                m.launch(s, s._ord(s._E), s._ord(s._H))
         _lib.call("fdtd_advance_many", ptr(self._steps), len(self.solvers), 1, stream)
         for s in self.solvers:
             s._issued += 1
@@ -186,19 +186,16 @@ class BatchSolver:
         plans = []
         for s, st in zip(self.solvers, self.streams):
             st.wait_event(fork)
-            plans.append([s.steps // s.graph_steps, s.steps % s.graph_steps])
+            plans.append(list(s._replays()))
         # round-robin graph replays, one per instance per round
-        while any(p[0] for p in plans):
+        while any(plans):
             for s, st, p in zip(self.solvers, self.streams, plans):
-                if p[0]:
+                if p:
                     with torch.cuda.stream(st):
-                        s.graphs[s.graph_steps].replay()
-                    p[0] -= 1
-        for s, st, p in zip(self.solvers, self.streams, plans):
-            if p[1]:
-                with torch.cuda.stream(st):
-                    s.graphs[p[1]].replay()
+                        p.pop(0).replay()
+        for s in self.solvers:
             s._issued = s.steps
+            s._rel ^= s._final_flip
             for m in s.monitors:
                 m._folded = s.steps
         for st in self.streams:

@@ -132,12 +132,17 @@ class Monitor:
         if into is None:
             self._folded = issued
 
-    def launch(self, s):
+    def launch(self, s, E=None, H=None):
+        """Record the step just computed; E, H are the (entry 0, entry 1)
+        pointer pairs the recorder picks from by the step parity (default:
+        the solver's field buffers)."""
         if self.shared is not None:
             return
         nx, ny, nz = s.shape
         stream = _lib.stream_handle(s.device)
-        common = (ptr(s._E[0]), ptr(s._E[1]), ptr(s._H[0]), ptr(s._H[1]), ptr(s.step))
+        E = E or s._ord(s._E)
+        H = H or s._ord(s._H)
+        common = (E[0], E[1], H[0], H[1], ptr(s.step))
         steps = int(self.indices.numel())
         if self.is_phasor:
             _lib.call(

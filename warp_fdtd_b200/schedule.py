@@ -10,6 +10,11 @@ so that every resident block slot of the GPU gets one run: one wave, no tail.
 
 `balanced_schedule` returns the (blocks, 4) int32 table of
 `fdtd_step_args.schedule`: (y tile index, first plane, end plane, 0).
+
+`segment_schedule` balances the time-blocked kernel (fdtd_step_block), which
+runs one block per SM: with so few blocks per tile, whole runs per tile
+quantise badly, so a block's planes may continue into the next tile (a second
+segment) and every block gets the same estimated cost.
 """
 
 import numpy as np
@@ -86,3 +91,39 @@ def batch_schedule(grids, tile_y, blocks, wy=Y_WEIGHT, wx=X_WEIGHT, max_run=MAX_
             cuts = [0] + [int(np.searchsorted(cum, cum[-1] * k / n)) for k in range(1, n)] + [nx]
             entries += [(g, t, a, b) for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
     return np.asarray(entries, np.int32).reshape(-1, 4)
+
+
+def segment_schedule(shape, tile_y, coeff_e, coeff_h, blocks, wy=Y_WEIGHT, wx=X_WEIGHT,
+                     segment_cost=2.0):
+    """Cut the tiles' planes, taken tile after tile, into `blocks` consecutive
+    pieces of equal estimated cost; a piece crossing a tile boundary becomes
+    several segments of its block, each charged `segment_cost` planes for its
+    pipeline start and halo planes.  Returns ((blocks * M, 4) int32 entries
+    (tile, first plane, end plane, 0), with tile -1 padding a block's list, and
+    M, the most segments of a block)."""
+    cost = plane_costs(shape, tile_y, coeff_e, coeff_h, wy, wx)
+    tiles, nx = cost.shape
+    blocks = max(1, min(int(blocks), tiles * nx))
+    # a tile change costs segment_cost planes of the tile's average plane
+    flat = cost.copy()
+    flat[:, 0] += segment_cost * cost.mean(axis=1)
+    cum = np.concatenate([[0.0], np.cumsum(flat.ravel())])
+    cuts = np.searchsorted(cum, cum[-1] * np.arange(blocks + 1) / blocks)
+    cuts[0], cuts[-1] = 0, tiles * nx
+    cuts = np.maximum.accumulate(cuts)
+    lists = []
+    for a, b in zip(cuts[:-1], cuts[1:]):
+        segs = []
+        while a < b:
+            t, xa = divmod(int(a), nx)
+            xb = min(nx, xa + int(b - a))
+            segs.append((t, xa, xb, 0))
+            a += xb - xa
+        lists.append(segs)
+    lists = [s for s in lists if s]
+    M = max(len(s) for s in lists)
+    out = np.full((len(lists), M, 4), -1, np.int32)
+    out[..., 3] = 0
+    for i, segs in enumerate(lists):
+        out[i, :len(segs)] = segs
+    return out.reshape(-1, 4), M

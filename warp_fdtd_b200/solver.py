@@ -25,7 +25,7 @@ import torch
 
 from . import _lib
 from . import kernels as k
-from .schedule import X_WEIGHT, Y_WEIGHT, balanced_schedule
+from .schedule import X_WEIGHT, Y_WEIGHT, balanced_schedule, segment_schedule
 from ._lib import ptr
 from .bundle import read_bundle
 
@@ -147,7 +147,7 @@ SUPPORTED_PROFILES = ("SingleFrequencyProfile", "GaussianPulseProfile", "HannPul
 
 class Solver:
     def __init__(self, case, device="cuda:0", graph_steps=64, cpml_storage="full",
-                 material="auto", tile=None, path=0, schedule="balanced"):
+                 material="auto", tile=None, path=0, schedule="balanced", time_block="auto"):
         if cpml_storage not in ("full", "packed"):
             raise ValueError("cpml_storage must be full or packed")
         if material not in ("auto", "u8", "f32"):
@@ -212,6 +212,9 @@ class Solver:
         self._issued = 0
         self.step = torch.zeros(1, dtype=torch.int32, device=dev)
         self._advance_counter = torch.zeros(1, dtype=torch.int32, device=dev)
+        # status word of the step kernels: 0, or 1 (a bounded wait expired),
+        # 2 (CPML ranks break the slab layout), 3 (bad schedule entry)
+        self.kernel_status = torch.zeros(1, dtype=torch.int32, device=dev)
 
         # materials: uint8 index + table when possible, else float32 per cell
         flat = np.ascontiguousarray(eps.reshape(-1), np.float32)
@@ -319,6 +322,26 @@ class Solver:
         self.save_h_from = self.steps
         self.graphs = {}
         self._args = self._step_args()
+        # time-blocked kernel (fdtd_step_block): single steps at depth 1 and,
+        # with time_block 2, pairs of steps in one launch inside run()
+        if time_block not in ("auto", 0, 1, 2):
+            raise ValueError("time_block must be 'auto', 0, 1 or 2")
+        self.time_block = 0
+        if self._psi_layout == 2 and time_block != 0:
+            self.time_block = 2 if time_block == "auto" else int(time_block)
+        # Physical buffer j of E, H and the CPML state is passed to the
+        # kernels as pair entry j ^ _rel: a two-step launch moves the state
+        # to the other buffer while the step parity stays, so it flips _rel.
+        self._rel = 0
+        self._final_flip = 0
+        self._block = {}
+        # launch shape of the time-blocked kernel per depth: (tile rows, TMA
+        # stages), 0 = the library's pick
+        self.block_shape = {1: (0, 0), 2: (0, 0)}
+        self._mid = None
+        self._extra2 = None
+        if self.time_block:
+            self._block_setup()
 
     # -- buffers selected by the number of issued steps --------------------
     def _compact(self, buf, rows):
@@ -330,16 +353,16 @@ class Solver:
 
     @property
     def E(self):
-        return self._compact(self._E[self._issued & 1], 3)
+        return self._compact(self._E[(self._issued & 1) ^ self._rel], 3)
 
     @property
     def H(self):
-        return self._compact(self._H[self._issued & 1], 3)
+        return self._compact(self._H[(self._issued & 1) ^ self._rel], 3)
 
     @property
     def hprev(self):
         """H(n-1/2) after the last issued step (zeros before the first)."""
-        return self._compact(self._H[(self._issued + 1) & 1], 3)
+        return self._compact(self._H[((self._issued + 1) & 1) ^ self._rel], 3)
 
     def _psi_reference(self, buf, field):
         """CPML state in the reference layout: (6, n) by cell for
@@ -378,11 +401,11 @@ class Solver:
 
     @property
     def psi_e(self):
-        return self._psi_reference(self._psi_e[self._issued & 1], "E")
+        return self._psi_reference(self._psi_e[(self._issued & 1) ^ self._rel], "E")
 
     @property
     def psi_h(self):
-        return self._psi_reference(self._psi_h[self._issued & 1], "H")
+        return self._psi_reference(self._psi_h[(self._issued & 1) ^ self._rel], "H")
 
     def _sync_eps(self):
         """Copy `eps` (n,) into the padded float32 material the kernel reads."""
@@ -423,6 +446,7 @@ class Solver:
         a.tile_y, a.tile_z, a.chunk_x = (int(v) for v in self.tile)
         a.stages = self.stages
         a.path = int(self.kernel_path)
+        a.error = ptr(self.kernel_status)
         self._schedule = None
         if self._psi_layout == 2 and self.schedule == "balanced" and a.chunk_x <= 0:
             # one wave of cost-balanced (tile, x run) blocks, see schedule.py
@@ -446,15 +470,21 @@ class Solver:
         return a
 
     def autotune(self, tiles=None, stages=(3, 2), weights=None, repeats=20):
-        """Pick the fused step's launch shape by timing it on this grid.
+        """Pick the step's launch shape by timing it on this grid.
 
-        Every candidate (tile rows, TMA stages, schedule cost weights) is timed
-        over `repeats` fused steps with CUDA events after a warm-up; the
-        fastest is kept.  Candidates that do not fit (shared memory, threads)
-        are skipped.  The solver is reset afterwards.  Returns the timings
-        {(tile_y, stages, weights): ms}.  Only the full-z path is tuned."""
+        With the time-blocked kernel (time_block 1 or 2) the candidates are
+        (temporal depth, tile rows, TMA stages): each is timed over `repeats`
+        launches with CUDA events after a warm-up, as milliseconds per time
+        step (a depth-2 launch counts two), and the fastest is kept, depth
+        included (time_block drops to 1 when single steps win).  Otherwise the
+        single-step kernel's (tile rows, TMA stages, schedule cost weights) are
+        tuned.  Candidates that do not fit (shared memory, threads) are
+        skipped.  The solver is reset afterwards.  Returns the timings
+        {candidate: ms per step}."""
         if self._psi_layout != 2:
             raise ValueError("autotune tunes the full-z path (path 0 or 3)")
+        if self.time_block:
+            return self._autotune_block(tiles, stages, repeats)
         a = self._step_args()
         _lib.call("fdtd_step_defaults", ctypes.byref(a))
         base = int(a.tile_y)
@@ -491,6 +521,58 @@ class Solver:
         self.reset()
         return timings
 
+    def _autotune_block(self, tiles, stages, repeats):
+        stream = torch.cuda.current_stream(self.device)
+        depths = (1, 2) if self.time_block == 2 else (1,)
+        saved = (self.time_block, dict(self.block_shape))
+        timings = {}
+        for depth in depths:
+            self.time_block = max(depths)
+            auto = self._block[depth]["plan"].tile_y
+            cands = tiles or sorted({max(1, auto - 2), max(1, auto - 1), auto, auto + 1})
+            for ty in cands:
+                for st in stages:
+                    try:
+                        self.set_block_shape(depth, ty, st)
+                    except (ValueError, _lib.FdtdError):
+                        continue
+                    info = self._block[depth]
+                    extra = self._pair_extra() if depth == 2 else info["extra"]
+                    if extra is None:
+                        continue
+
+                    def launch():
+                        _lib.call("fdtd_step_block", ctypes.byref(info["args"][self._rel]),
+                                  ctypes.byref(info["plan"]), ctypes.byref(extra),
+                                  stream.cuda_stream)
+
+                    for _ in range(3):
+                        launch()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record(stream)
+                    for _ in range(repeats):
+                        launch()
+                    e1.record(stream)
+                    e1.synchronize()
+                    timings[(depth, ty, st)] = e0.elapsed_time(e1) / repeats / depth
+            self.block_shape[depth] = saved[1][depth]
+        if timings:
+            best = min(timings, key=timings.get)
+            for depth in depths:  # each depth keeps its own fastest shape
+                own = {c: v for c, v in timings.items() if c[0] == depth}
+                if own:
+                    d, ty, st = min(own, key=own.get)
+                    self.block_shape[depth] = (ty, st)
+            self.time_block = best[0]
+        else:
+            self.time_block, self.block_shape = saved
+        self._block_setup()
+        self._extra2 = None
+        self.graphs = {}
+        self.reset()
+        return timings
+
     def set_tile(self, tile_y, tile_z, chunk_x=0, stages=0):
         """Change the fused kernel's launch shape (tile rows, tile z cells,
         planes per block with 0 for the schedule, TMA ring stages with 0 for the
@@ -498,6 +580,17 @@ class Solver:
         self.tile = (int(tile_y), int(tile_z), int(chunk_x))
         self.stages = int(stages)
         self._args = self._step_args()
+        self.graphs = {}
+
+    def set_block_shape(self, depth, tile_y=0, stages=0):
+        """Launch shape of the time-blocked kernel at `depth` (1 or 2): tile
+        rows and TMA stages, 0 for the library's pick; captured graphs are
+        dropped."""
+        if depth not in (1, 2) or not self.time_block or depth > self.time_block:
+            raise ValueError("set_block_shape: depth not enabled by this solver's time_block")
+        self.block_shape[depth] = (int(tile_y), int(stages))
+        self._block_setup()
+        self._extra2 = None
         self.graphs = {}
 
 
@@ -513,28 +606,121 @@ class Solver:
                 a.zero_()
         self.step.zero_()
         self._issued = 0
+        self._rel = 0
         for monitor in self.monitors:
             monitor.reset()
         torch.cuda.synchronize(self.device)
 
-    def launch_step(self):
-        """One step: fused E+H update, detectors, advance (solver.py:194-237)."""
-        if self._issued >= self.steps and not torch.cuda.is_current_stream_capturing():
-            raise ValueError("Trajectory complete; call reset() before stepping again")
-        stream = _lib.stream_handle(self.device)
-        _lib.call("fdtd_step_fused", self._args, stream)
-        self._after_update(stream)
+    # -- time-blocked kernel ------------------------------------------------
+    def _block_setup(self):
+        """Plans, schedules and argument pairs of the time-blocked kernel."""
+        ce = self._coeff_step["E"].cpu().numpy()
+        ch = self._coeff_step["H"].cpu().numpy()
+        for depth in ((1, 2) if self.time_block == 2 else (1,)):
+            base = self._step_args()
+            base.schedule, base.schedule_blocks = None, 0
+            base.tile_y, base.stages = (int(v) for v in self.block_shape[depth])
+            base.chunk_x = 0
+            plan = _lib.BlockPlan()
+            _lib.call("fdtd_step_block_prepare", ctypes.byref(base), depth, ctypes.byref(plan))
+            slots = max(1, plan.blocks_per_sm) * max(1, plan.sms)
+            runs, segments = segment_schedule(self.shape, plan.tile_y, ce, ch, slots,
+                                              *self.schedule_weights)
+            nblocks = runs.shape[0] // segments
+            sched = torch.from_numpy(runs).to(self.device)
+            base.tile_y = plan.tile_y
+            base.schedule = ptr(sched)
+            base.schedule_blocks = int(nblocks)
+            real = runs[runs[:, 0] >= 0]
+            base.chunk_x = int((real[:, 2] - real[:, 1]).max())
+            pair = [base, self._swapped(base)]
+            extra = _lib.BlockExtra()
+            extra.segments = int(segments)
+            scratch = None
+            if depth == 2:
+                nbytes = int(plan.scratch_block_bytes) * int(nblocks)
+                scratch = torch.empty(max(1, nbytes // 4), dtype=torch.float32, device=self.device)
+                extra.scratch = ptr(scratch)
+                extra.scratch_bytes = nbytes
+            self._block[depth] = {"plan": plan, "schedule": sched, "args": pair,
+                                  "extra": extra, "scratch": scratch}
+
+    @staticmethod
+    def _swapped(a):
+        b = _lib.StepArgs()
+        ctypes.pointer(b)[0] = a
+        for name in ("E", "H", "psi_e", "psi_h"):
+            pa, pb = getattr(a, name), getattr(b, name)
+            pb[0], pb[1] = pa[1], pa[0]
+        return b
+
+    def _ord(self, bufs):
+        """The (entry 0, entry 1) pointers of a physical buffer pair as the
+        kernels' parity convention sees them now."""
+        return ptr(bufs[self._rel]), ptr(bufs[self._rel ^ 1])
+
+    def _pair_extra(self):
+        """Depth-2 extras: scratch plus the snapshot boxes the detectors
+        sample; None when the attached monitors cannot be fed from a
+        snapshot (then run() advances one step per launch)."""
+        key = tuple(id(m) for m in self.monitors)
+        if self._extra2 is not None and self._extra2[0] == key:
+            return self._extra2[1]
+        boxes, ok = [], True
+        nx, ny, nz = self.shape
+        for m in self.monitors:
+            if getattr(m, "shared", None) is not None:
+                continue
+            lo, shape = getattr(m, "lo", None), getattr(m, "shape", None)
+            if lo is None or not hasattr(m, "exact") or type(m).__name__ != "Monitor":
+                ok = False
+                break
+            e = 1 if m.exact else 0
+            box = [max(lo[0] - e, 0), lo[0] + shape[0], max(lo[1] - e, 0), lo[1] + shape[1],
+                   lo[2], min(lo[2] + shape[2] + e, nz)]
+            boxes.append(box)
+        extra = None
+        if ok and len(boxes) <= _lib.SNAP_BOXES_MAX:
+            info = self._block[2]
+            extra = _lib.BlockExtra()
+            extra.scratch = info["extra"].scratch
+            extra.scratch_bytes = info["extra"].scratch_bytes
+            extra.segments = info["extra"].segments
+            if boxes:
+                if self._mid is None:
+                    f32 = dict(dtype=torch.float32, device=self.device)
+                    self._mid = (torch.zeros((3, self._cells), **f32),
+                                 torch.zeros((3, self._cells), **f32))
+                extra.snap_e, extra.snap_h = ptr(self._mid[0]), ptr(self._mid[1])
+                extra.nsnap = len(boxes)
+                for b, box in enumerate(boxes):
+                    for j, v in enumerate(box):
+                        extra.snap_box[b][j] = int(v)
+        self._extra2 = (key, extra)
+        return extra
+
+    def _step_kernel(self, stream):
+        """One fused step of the current buffers (no detectors, no advance)."""
+        if self.time_block:
+            info = self._block[1]
+            _lib.call("fdtd_step_block", ctypes.byref(info["args"][self._rel]),
+                      ctypes.byref(info["plan"]), ctypes.byref(info["extra"]), stream)
+        else:
+            _lib.call("fdtd_step_fused", self._args, stream)
+
+    def _record(self, E, H, stream):
+        """Detectors of the step just computed (E, H: the (entry 0, entry 1)
+        pointer pairs they read) and the counter advance."""
         planes, grouped = self._staged_planes()
         for monitor in self.monitors:
             if id(monitor) not in grouped:
-                monitor.launch(self)
+                monitor.launch(self, E, H)
         if grouped:
             # every staged phasor plane in one launch, which also advances the
             # step counter after all of its blocks have read it
             nx, ny, nz = self.shape
-            _lib.call("fdtd_record_stage_many", ptr(self._E[0]), ptr(self._E[1]),
-                      ptr(self._H[0]), ptr(self._H[1]), ptr(self.step), planes, len(planes),
-                      nx, ny, nz, self._pitch, ptr(self._advance_counter), 1, stream)
+            _lib.call("fdtd_record_stage_many", E[0], E[1], H[0], H[1], ptr(self.step), planes,
+                      len(planes), nx, ny, nz, self._pitch, ptr(self._advance_counter), 1, stream)
         else:
             _lib.call("fdtd_advance", ptr(self.step), 1, stream)
         self._issued += 1
@@ -542,6 +728,50 @@ class Solver:
             if monitor.is_phasor and (self._issued % monitor.batch == 0
                                       or self._issued == self.steps):
                 monitor.fold(self, self._issued)
+
+    def launch_step(self):
+        """One step: fused E+H update, detectors, advance (solver.py:194-237)."""
+        if self._issued >= self.steps and not torch.cuda.is_current_stream_capturing():
+            raise ValueError("Trajectory complete; call reset() before stepping again")
+        stream = _lib.stream_handle(self.device)
+        self._step_kernel(stream)
+        self._after_update(stream)
+        self._record(self._ord(self._E), self._ord(self._H), stream)
+
+    def _launch_pair(self, extra):
+        """Two steps in one launch (depth 2), then the detectors of both: the
+        first reads the snapshot of E(n+1), H(n+1/2), the second reads it as
+        H(n-1/2)."""
+        stream = _lib.stream_handle(self.device)
+        info = self._block[2]
+        _lib.call("fdtd_step_block", ctypes.byref(info["args"][self._rel]),
+                  ctypes.byref(info["plan"]), ctypes.byref(extra), stream)
+        s = self._issued & 1
+        cur = s ^ self._rel  # physical buffer of the input state
+        midE = ptr(self._mid[0]) if self._mid is not None else ptr(self._E[cur ^ 1])
+        midH = ptr(self._mid[1]) if self._mid is not None else ptr(self._H[cur ^ 1])
+        # step t (parity s) samples E[s^1], H[s^1] and H(n-1/2) = H[s]; step
+        # t+1 (parity s^1) samples E[s], H[s] and H(n+1/2) = H[s^1]
+        for src in (cur, cur ^ 1):
+            E, H = [None, None], [None, None]
+            E[s], E[s ^ 1] = ptr(self._E[src]), midE
+            H[s], H[s ^ 1] = ptr(self._H[src]), midH
+            self._record(E, H, stream)
+        self._rel ^= 1
+
+    def _segment(self, length, final):
+        """Issue `length` steps: pairs where the time-blocked kernel runs them,
+        an even number of pairs unless `final` (the trajectory's last segment,
+        which ends with a single step so that hprev is H(n-1/2))."""
+        extra = self._pair_extra() if self.time_block == 2 else None
+        n2 = 0
+        if extra is not None:
+            n2 = (length - 1) // 2 if final else 2 * (length // 4)
+        for _ in range(n2):
+            self._launch_pair(extra)
+        for _ in range(length - 2 * n2):
+            self.launch_step()
+        return n2
 
     def _after_update(self, stream):
         """Hook between the fused update and the detectors (the step counter
@@ -568,41 +798,84 @@ class Solver:
                 self._staged = (planes, frozenset(key))
         return self._staged
 
+    def _graph_segments(self):
+        """Graph segments of a whole trajectory: (key, length, start, final).
+
+        A pair's detector launches are captured for the step parity at its
+        start, so with an odd graph_steps the full graphs (which then start
+        on both parities) are captured once per starting parity."""
+        G, N = self.graph_steps, self.steps
+        if self.time_block == 2:
+            last = N % G or min(G, N)
+            full = (N - last) // G
+            segs = [(("full", c & 1), G, c * G, False) for c in range(min(full, 2 if G & 1 else 1))]
+            return segs + [("final", last, N - last, True)]
+        return [(length, length, 0 if length == G else N - length, False)
+                for length in sorted({G, N % G} - {0}) if length <= N]
+
+    def step_launches(self):
+        """(two-step launches, one-step launches) of a whole trajectory run
+        through the captured graphs."""
+        if self.time_block != 2 or self._pair_extra() is None:
+            return 0, self.steps
+        G, N = self.graph_steps, self.steps
+        last = N % G or min(G, N)
+        full = (N - last) // G
+        pairs = full * 2 * (G // 4) + (last - 1) // 2
+        return pairs, N - 2 * pairs
+
+    def _replays(self):
+        """The captured graphs of a whole trajectory, in replay order."""
+        G, N = self.graph_steps, self.steps
+        if self.time_block == 2:
+            last = N % G or min(G, N)
+            return ([self.graphs[("full", (c * G) & 1)] for c in range((N - last) // G)]
+                    + [self.graphs["final"]])
+        out = [self.graphs[G]] * (N // G)
+        if N % G:
+            out.append(self.graphs[N % G])
+        return out
+
     def compile(self):
         start = time.perf_counter()
         with torch.cuda.device(self.device):
+            if self.time_block == 2:
+                self._pair_extra()  # buffers are allocated before any capture
             self.launch_step()
             torch.cuda.synchronize(self.device)
             self.reset()
-            for length in {self.graph_steps, self.steps % self.graph_steps} - {0}:
+            self._final_flip = 0
+            for key, length, offset, final in self._graph_segments():
                 # capture at the step offset where the graph will be replayed so
                 # the detectors' folds land on the right steps: full graphs start
-                # on multiples of graph_steps, the tail graph ends the trajectory
-                start = 0 if length == self.graph_steps else self.steps - length
-                self._issued = start
+                # on multiples of graph_steps, the last graph ends the trajectory
+                self._issued = offset
+                self._rel = 0
                 for m in self.monitors:
-                    m._folded = start
+                    m._folded = offset
                 g = torch.cuda.CUDAGraph()
                 with torch.cuda.graph(g, capture_error_mode="relaxed"):
-                    for _ in range(length):
-                        self.launch_step()
+                    n2 = self._segment(length, final) if self.time_block == 2 else 0
+                    if self.time_block != 2:
+                        for _ in range(length):
+                            self.launch_step()
+                if final:
+                    self._final_flip = n2 & 1
                 self._issued = 0
-                self.graphs[length] = g
+                self._rel = 0
+                self.graphs[key] = g
             self.reset()
         return time.perf_counter() - start
 
     def run(self):
         with torch.cuda.device(self.device):
             if not self.graphs:
-                for _ in range(self.steps - self._issued):
-                    self.launch_step()
+                self._segment(self.steps - self._issued, final=True)
             else:
-                for _ in range(self.steps // self.graph_steps):
-                    self.graphs[self.graph_steps].replay()
-                tail = self.steps % self.graph_steps
-                if tail:
-                    self.graphs[tail].replay()
+                for g in self._replays():
+                    g.replay()
                 self._issued += self.steps
+                self._rel ^= self._final_flip
                 for m in self.monitors:
                     m._folded = self.steps
             torch.cuda.synchronize(self.device)
@@ -620,7 +893,7 @@ class Solver:
             if arr is None:
                 continue
             src = torch.as_tensor(np.asarray(arr, np.float32)).reshape(3, nx, ny, nz)
-            dst = bufs[self._issued & 1].view(3, nx, ny, self._pitch)
+            dst = bufs[(self._issued & 1) ^ self._rel].view(3, nx, ny, self._pitch)
             dst[..., :nz].copy_(src.to(self.device))
 
     def summary(self):

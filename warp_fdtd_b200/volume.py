@@ -50,9 +50,11 @@ class VolumeMonitor:
         solver.monitors.append(self)
         solver.save_h_from = min(solver.save_h_from, self.first)
 
-    def launch(self, s):
+    def launch(self, s, E=None, H=None):
         nx, ny, nz = s.shape
-        _lib.call("fdtd_record_volume", ptr(s._E[0]), ptr(s._E[1]), ptr(s._H[0]), ptr(s._H[1]),
+        E = E or s._ord(s._E)
+        H = H or s._ord(s._H)
+        _lib.call("fdtd_record_volume", E[0], E[1], H[0], H[1],
                   ptr(s.step), ptr(self.positions), self.n, ptr(self.weights),
                   int(self.weights.shape[0]), int(self.first), ptr(self.phasor), nx, ny, nz,
                   s._pitch, _lib.stream_handle(s.device))
