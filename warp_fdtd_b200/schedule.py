@@ -29,6 +29,13 @@ MAX_RUN = 96
 Y_WEIGHT = 0.9
 X_WEIGHT = 0.7
 
+# The same for the time-blocked kernel (fdtd_step_block), and the cost of a
+# block's extra segment in planes: a least-squares fit of per-block durations
+# (globaltimer at block start and end) on the 20 nm bend at depth 2, tile 7.
+BLOCK_Y_WEIGHT = 0.61
+BLOCK_X_WEIGHT = 0.60
+BLOCK_SEGMENT_COST = 2.9
+
 
 def plane_costs(shape, tile_y, coeff_e, coeff_h, wy=Y_WEIGHT, wx=X_WEIGHT):
     """(tiles, nx) estimated cost of each tile plane; coeff_* are the (3, L, 4)

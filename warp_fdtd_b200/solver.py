@@ -25,7 +25,8 @@ import torch
 
 from . import _lib
 from . import kernels as k
-from .schedule import X_WEIGHT, Y_WEIGHT, balanced_schedule, segment_schedule
+from .schedule import (BLOCK_SEGMENT_COST, BLOCK_X_WEIGHT, BLOCK_Y_WEIGHT, X_WEIGHT, Y_WEIGHT,
+                       balanced_schedule, segment_schedule)
 from ._lib import ptr
 from .bundle import read_bundle
 
@@ -625,7 +626,7 @@ class Solver:
             _lib.call("fdtd_step_block_prepare", ctypes.byref(base), depth, ctypes.byref(plan))
             slots = max(1, plan.blocks_per_sm) * max(1, plan.sms)
             runs, segments = segment_schedule(self.shape, plan.tile_y, ce, ch, slots,
-                                              *self.schedule_weights)
+                                              BLOCK_Y_WEIGHT, BLOCK_X_WEIGHT, BLOCK_SEGMENT_COST)
             nblocks = runs.shape[0] // segments
             sched = torch.from_numpy(runs).to(self.device)
             base.tile_y = plan.tile_y
