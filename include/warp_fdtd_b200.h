@@ -184,7 +184,10 @@ int fdtd_material_forward(const float *p, const float *weights, int radius, floa
  * every GPU that loads the library until the process exits); px * py above
  * that limit is rejected with FDTD_ERR_ARG.  The first call on a device looks
  * up the array's device address (cudaGetSymbolAddress) with that device
- * current, so make that first call before any stream capture.  Every call
+ * current, so make that first call before any stream capture.  The address
+ * is kept for the life of the process: do not use this entry point on a
+ * device after cudaDeviceReset (or any teardown of its primary context) in
+ * the same process.  Every call
  * shares the one array: calls whose work overlaps on the GPU (other streams,
  * other threads) race and must be serialised by the caller.  Nothing in the
  * array needs clearing between calls; each call overwrites the px * py
@@ -303,7 +306,10 @@ int fdtd_batch_prepare(const fdtd_step_args *args, int count, void *workspace,
 int fdtd_step_batch(const fdtd_batch_plan *plan, const void *workspace, const int *schedule,
                     int blocks, void *stream);
 int fdtd_advance_many(int *const *steps, int count, int delta, void *stream);
-/* Free a prepared batch's parameter slots (the workspace is the caller's). */
+/* Free a prepared batch's parameter slots (the workspace is the caller's).
+ * No fdtd_step_batch launch of the plan may still be pending on the device:
+ * a later fdtd_batch_prepare can take the slots and rewrite them at once.
+ * fdtd_step_batch must run with the plan's device current. */
 int fdtd_batch_release(fdtd_batch_plan *plan);
 
 /* Time-blocked fused step: one launch advances E and H by `depth` (1 or 2)

@@ -128,3 +128,31 @@ def test_surrogate_and_reverse_entry_points_reject_bad_arguments(lib):
                                0.5, 0, 0, 0, 0, 0, 0, None) == -1  # electric half needs eps
     assert L.fdtd_reverse_half(1, 16, 32, 48, 64, 80, 96, 8, 112, 128, 144, 160, 4, 4, 4, 0.5,
                                2, 0, 0, 4, 4, 4, None) == -1  # design box outside the grid
+
+
+def test_inject_many_and_block_step_reject_bad_arguments(lib):
+    """fdtd_inject_many and the time-blocked step check their arguments on
+    the host, before any launch."""
+    from warp_fdtd_b200 import _lib
+
+    L = _lib.load()
+    planes = (_lib.InjectPlane * 9)()
+    for pl in planes:
+        pl.source, pl.weights, pl.sx, pl.sy, pl.sz = 16, 32, 1, 2, 2
+    args = (16, 32)
+    assert L.fdtd_inject_many(*args, planes, 9, 48, 4, 4, 4, 0, None) == -1  # > 8 planes
+    assert L.fdtd_inject_many(*args, planes, 0, 48, 4, 4, 4, 0, None) == -1  # no plane
+    planes[1].source = None
+    assert L.fdtd_inject_many(*args, planes, 2, 48, 4, 4, 4, 0, None) == -1  # null source
+    assert b"plane 1" in L.fdtd_last_error()
+    planes[1].source, planes[1].sy = 16, 0
+    assert L.fdtd_inject_many(*args, planes, 2, 48, 4, 4, 4, 0, None) == -1  # empty extent
+    assert L.fdtd_inject_many(None, 32, planes, 1, 48, 4, 4, 4, 0, None) == -1  # null field
+    a = _lib.StepArgs()
+    plan = _lib.BlockPlan()
+    assert L.fdtd_step_block_prepare(ctypes.byref(a), 3, ctypes.byref(plan)) == -1  # depth 3
+    assert L.fdtd_step_block_prepare(None, 2, ctypes.byref(plan)) == -1
+    assert L.fdtd_step_block_prepare(ctypes.byref(a), 2, ctypes.byref(plan)) == -1  # empty grid
+    assert L.fdtd_step_block(ctypes.byref(a), None, None, None) == -1
+    plan.depth = 2
+    assert L.fdtd_step_block(ctypes.byref(a), ctypes.byref(plan), None, None) == -1

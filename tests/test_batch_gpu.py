@@ -144,3 +144,49 @@ def test_batch_adjoint_matches_single_instances(tmp_path):
     for (l0, g0), (l1, g1) in zip(single, batched):
         assert l0 == l1
         assert np.linalg.norm(g1 - g0) / np.linalg.norm(g0) < 1e-5
+
+
+def test_batch_release_with_launches_queued_and_device_check(tmp_path):
+    """A fused batch closed while its steps are still queued (no synchronise)
+    keeps its results: close() waits before the parameter slots go back, and
+    a second batch prepared at once on the same slots does not disturb the
+    first.  A plan is refused on a device other than its own."""
+    import copy
+    import ctypes
+
+    from tests.bundles import make_bundle
+    from warp_fdtd_b200 import _lib
+    from warp_fdtd_b200.batch import BatchSolver
+    from warp_fdtd_b200.solver import Solver
+
+    shapes = [(14, 12, 28), (23, 9, 28)]
+    cases = [make_bundle(tmp_path / f"r{i}", sh, 20, seed=40 + i) for i, sh in enumerate(shapes)]
+    steps = 9
+    alone = []
+    for c in cases:
+        s = Solver(c)
+        s.reset()
+        for _ in range(steps):
+            s.launch_step()
+        alone.append(s.fields())
+    first = [Solver(c) for c in cases]
+    batch = BatchSolver(first, fused=True)
+    assert batch.fused
+    batch.reset()
+    for _ in range(steps):
+        batch.launch_step()  # queued, not synchronised
+    batch.close()
+    second = BatchSolver([Solver(c) for c in reversed(cases)], fused=True)
+    second.reset()
+    for _ in range(3):
+        second.launch_step()
+    torch.cuda.synchronize()
+    for s, want in zip(first, alone):
+        np.testing.assert_array_equal(s.fields()["E"], want["E"])
+        np.testing.assert_array_equal(s.fields()["H"], want["H"])
+    plan = copy.copy(second._plan)
+    plan.device = plan.device + 1
+    with pytest.raises(ValueError, match="device"):
+        _lib.call("fdtd_step_batch", ctypes.byref(plan), second._ws, second._schedule.data_ptr(),
+                  second._blocks, _lib.stream_handle())
+    second.close()

@@ -451,3 +451,53 @@ def test_inject_matches_oracle():
         torch.cuda.synchronize()
         np.testing.assert_allclose(N(qe), qe_o, rtol=1e-6, atol=1e-6)
         np.testing.assert_allclose(N(qh), qh_o, rtol=1e-6, atol=1e-6)
+
+
+@pytest.mark.parametrize("nplanes", [2, 5, 8])
+def test_inject_many_matches_per_plane_oracle(nplanes):
+    """fdtd_inject_many over planes of uneven extents (some overlapping, some
+    on the grid's edge) equals the oracle's inject applied plane by plane,
+    within float32 atomic-order tolerance; a zero-weight step adds nothing."""
+    import ctypes
+
+    from warp_fdtd_b200 import _lib
+
+    rng = np.random.default_rng(30 + nplanes)
+    shape = (9, 11, 13)
+    nx, ny, nz = shape
+    n = int(np.prod(shape))
+    steps = 4
+    planes, keep = [], []
+    for k in range(nplanes):
+        sx, sy, sz = int(rng.integers(1, 4)), int(rng.integers(1, ny + 1)), int(rng.integers(1, nz + 1))
+        if k == 1:  # overlaps plane 0 exactly
+            (x0, y0, z0), (sx, sy, sz) = planes[0][0], planes[0][1]
+        else:
+            x0, y0, z0 = (int(rng.integers(0, d - s + 1)) for d, s in zip(shape, (sx, sy, sz)))
+        count = sx * sy * sz
+        src = rng.normal(size=(6, count, 2)).astype(np.float32)
+        w = rng.normal(size=(steps, 2)).astype(np.float32)
+        w[2] = 0.0  # a step without a source
+        planes.append(((x0, y0, z0), (sx, sy, sz), src, w))
+    for t in (1, 2):
+        for old in (0, 1):
+            qe_o = np.zeros((3, n), np.float32)
+            qh_o = np.zeros((3, n), np.float32)
+            for lo, sh, src, w in planes:
+                ocpu.inject(qe_o, qh_o, src, w, t, shape, lo, sh, old)
+            arr = (_lib.InjectPlane * nplanes)()
+            for pl, (lo, sh, src, w) in zip(arr, planes):
+                s_t, w_t = T(src), T(w)
+                keep += [s_t, w_t]
+                pl.source, pl.weights = s_t.data_ptr(), w_t.data_ptr()
+                pl.x0, pl.y0, pl.z0 = lo
+                pl.sx, pl.sy, pl.sz = sh
+            qe, qh = torch.zeros((3, n), device="cuda"), torch.zeros((3, n), device="cuda")
+            step = T(np.array([t], np.int32))
+            _lib.call("fdtd_inject_many", qe.data_ptr(), qh.data_ptr(), arr, nplanes,
+                      step.data_ptr(), nx, ny, nz, old, None)
+            torch.cuda.synchronize()
+            np.testing.assert_allclose(N(qe), qe_o, rtol=1e-5, atol=1e-5)
+            np.testing.assert_allclose(N(qh), qh_o, rtol=1e-5, atol=1e-5)
+            if t == 2:
+                assert not N(qe).any() and not N(qh).any()

@@ -93,9 +93,13 @@ class BatchSolver:
                                    device=self.device)
 
     def close(self):
-        """Free the batch's slots in the library's grid-parameter table."""
+        """Free the batch's slots in the library's grid-parameter table, once
+        the device has finished every launch that reads them (a batch run with
+        launches still queued, for instance after graph replays without a
+        synchronise, would otherwise read a later batch's parameters)."""
         plan = getattr(self, "_plan", None)
         if plan is not None and plan.count > 0:
+            torch.cuda.synchronize(self.device)
             _lib.call("fdtd_batch_release", ctypes.byref(plan))
 
     def __del__(self):

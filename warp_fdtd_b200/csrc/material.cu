@@ -314,8 +314,12 @@ int fdtd_material_backward(const float *p, const float *weights, int radius, con
     float *rho = scratch, *g_rho = scratch + n;
     int rc = fdtd_material_smooth(p, weights, radius, rho, px, py, stream);
     if (rc) return rc;
-    cudaMemsetAsync(g_rho, 0, n * sizeof(float), (cudaStream_t)stream);
-    cudaMemsetAsync(p_grad, 0, n * sizeof(float), (cudaStream_t)stream);
+    cudaError_t err = cudaMemsetAsync(g_rho, 0, n * sizeof(float), (cudaStream_t)stream);
+    if (err == cudaSuccess) err = cudaMemsetAsync(p_grad, 0, n * sizeof(float), (cudaStream_t)stream);
+    if (err != cudaSuccess) {
+        set_error("fdtd_material_backward: clearing the accumulators: %s", cudaGetErrorString(err));
+        return FDTD_ERR_CUDA;
+    }
     rc = fdtd_material_subpixel_adjoint(rho, g, g_rho, px, py, beta, eps_lo, contrast, stream);
     if (rc) return rc;
     return fdtd_material_smooth_adjoint(g_rho, weights, radius, p_grad, px, py, stream);

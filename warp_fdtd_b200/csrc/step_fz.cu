@@ -913,6 +913,18 @@ extern "C" int fdtd_step_batch(const fdtd_batch_plan *plan, const void *workspac
         set_error("fdtd_step_batch: invalid arguments");
         return FDTD_ERR_ARG;
     }
+    // the parameter slots and the workspace live on the plan's device
+    int dev = -1;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) {
+        set_error("fdtd_step_batch: %s", cudaGetErrorString(err));
+        return FDTD_ERR_CUDA;
+    }
+    if (dev != plan->device) {
+        set_error("fdtd_step_batch: the plan was prepared on device %d, device %d is current",
+                  plan->device, dev);
+        return FDTD_ERR_ARG;
+    }
     FzBatchKernel kern = fz_pick_batch(plan->material_kind, plan->stages, plan->vector,
                                        plan->full_rows != 0);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, plan->smem_bytes);
