@@ -95,3 +95,23 @@ def test_gradient_matches_central_differences(grad20):
     # smallest pixels at 0.12 and 0.18 (T moves by ~1e-6 there)
     assert rel(fd, g[pixels]) < 0.02
     assert np.median(err) < 0.01
+
+
+def test_transmission_loss_autograd_function(grad20):
+    """TransmissionLoss.apply(params, adjoint) is -T as a torch scalar, and
+    backward() leaves upstream x the adjoint gradient in params.grad (here
+    upstream 2.5 from loss * 2.5).  The forward is deterministic, so the loss
+    equals differentiate()'s bit for bit; the reverse sweep's float32 atomics
+    leave the gradient equal to ~1e-6."""
+    from warp_fdtd_b200.adjoint_driver import TransmissionLoss
+
+    adj, p0, loss, grad = grad20
+    params = torch.tensor(p0, dtype=torch.float32, requires_grad=True)
+    out = TransmissionLoss.apply(params, adj)
+    assert out.shape == () and out.dtype == torch.float32 and out.requires_grad
+    assert out.item() == np.float32(loss)
+    (out * 2.5).backward()
+    assert params.grad is not None and params.grad.shape == params.shape
+    got = params.grad.numpy() / 2.5
+    assert rel(got, grad) < 1e-5
+    assert float(np.abs(got).max()) > 0

@@ -15,11 +15,13 @@ benchmarks have no such bundle, so this module writes them in the same format
   slab), b = exp(-(sigma / kappa + alpha) dt / eps0) and
   a = sigma / (sigma kappa + kappa^2 alpha) (b - 1).  `cpml_arrays` reproduces
   the exported pml_a/pml_b/inv_kappa arrays of the reference bundles from
-  their manifest parameters (tests/test_scene.py);
-* a semi-vectorial finite-difference eigenmode of the guide cross-section for
-  the source and the mode detectors (the dominant transverse E component and
-  its H partner n_eff * E; parity with FDTDX's full-vectorial mode solver is
-  not claimed);
+  their manifest parameters (tests/test_oracle.py);
+* the TE0 eigenmode of the Yee grid itself on the guide's cross-section
+  (full-vectorial, the leapfrog's discrete curls with its numerical
+  dispersion) for the source, and the same mode passed through the
+  recorder's colocation for the mode detectors: on the straight guide the
+  source launches the grid's own mode, so modal T is 1 and the backward
+  overlap R is ~1e-8 (FDTDX's continuum mode solver is not reproduced);
 * pulsed sources (GaussianPulseProfile, HannPulseProfile) and K-frequency DFT
   detectors ("frequencies_hz").
 """
@@ -96,43 +98,164 @@ def add_cpml(arrays, objects, shape, cells, dt, dx, frequency_hz):
 
 # ---------------------------------------------------------------- modes
 
-def solve_mode(eps, d, wavelength, n_guess):
-    """Fundamental scalar mode of a 2-D permittivity map eps[u, v] (grid step
-    d): (d2/du2 + d2/dv2 + k0^2 eps) f = beta^2 f with zero boundary values.
-    Returns (n_eff, f) with f normalised to max |f| = 1 and positive."""
+def _forward_difference(nu, nv, d, along):
+    """Forward difference (f[next] - f) / d on an nu x nv grid flattened row
+    major, along u (0) or v (1), with zero beyond the last row / column."""
+    n = nu * nv
+    step = nv if along == 0 else 1
+    upper = np.ones(n - step)
+    if along == 1:
+        upper[np.arange(1, n) % nv == 0] = 0.0  # no wrap into the next row
+    return sp.diags([-np.ones(n), upper], [0, step], format="csr") / d
+
+
+def yee_mode(eps, d, dt, wavelength, horizontal=0, n_guess=None):
+    """Fundamental TE-like eigenmode of the Yee grid itself on a cross-section.
+
+    `eps[i, j]` is the permittivity of the cells of the plane, indexed by the
+    local transverse axes (u, v); the mode travels along w, with (u, v, w) a
+    cyclic permutation of (x, y, z) so that the Yee lattice reads the same:
+    Eu at (i+1/2, j), Ev at (i, j+1/2), Ew at (i, j) a half cell further in
+    w, Hu at (i, j+1/2), Hv at (i+1/2, j), both a half cell further in w, and
+    Hw at (i+1/2, j+1/2).  Every cell uses its one permittivity for all three
+    E components, as the solver's update does.
+
+    With fields ~ exp(i (w t - beta w)) the leapfrog's differences are exact
+    for k~ = 2 sin(w dt / 2) / (c dt) and beta~ = 2 sin(beta d / 2) / d, and
+    eliminating Ew, Hw (discrete div H = 0) leaves beta~^2 [Hu; Hv] =
+    P [Hu; Hv] with, for D_u, D_v the forward and -D^T the backward
+    differences,
+
+        P = [[k~^2 e + e D_v e^-1 B_v + B_u D_u,   B_u D_v - e D_v e^-1 B_u],
+             [B_v D_u - e D_u e^-1 B_v,   k~^2 e + B_v D_v + e D_u e^-1 B_u]].
+
+    So the profile is the discrete mode of the update itself, not of
+    Maxwell's equations: a source built from it launches (almost) nothing
+    else, and a detector overlap with it rejects the backward mode.
+
+    TE-like means the E component along the local axis `horizontal` (0: u,
+    1: v) dominates, so the vertical H (the other local axis) dominates H.
+
+    Returns (beta, E, H): the true propagation constant (rad/m) and the
+    (3, nu, nv) complex phasors in local components (u, v, w), each at its
+    own Yee position; the transverse parts are real, Ew and Hw imaginary."""
     nu, nv = eps.shape
-    k0 = 2 * math.pi / wavelength
-    main = np.full(nu * nv, -4.0 / d ** 2) + k0 ** 2 * eps.ravel()
-    off_v = np.full(nu * nv - 1, 1.0 / d ** 2)
-    off_v[np.arange(1, nu * nv) % nv == 0] = 0.0
-    off_u = np.full(nu * nv - nv, 1.0 / d ** 2)
-    A = sp.diags([main, off_v, off_v, off_u, off_u], [0, 1, -1, nv, -nv], format="csc")
-    sigma = (k0 * n_guess) ** 2
-    vals, vecs = spla.eigs(A, k=1, sigma=sigma, which="LM")
-    beta2 = float(np.real(vals[0]))
-    f = np.real(vecs[:, 0]).reshape(nu, nv)
-    f /= f[np.unravel_index(np.argmax(np.abs(f)), f.shape)]
-    return math.sqrt(max(beta2, 0.0)) / k0, f
+    omega = 2 * math.pi * C0 / wavelength
+    k = 2 * math.sin(omega * dt / 2) / (C0 * dt)
+    e = sp.diags(eps.ravel().astype(np.float64))
+    ie = sp.diags(1.0 / eps.ravel().astype(np.float64))
+    Du, Dv = _forward_difference(nu, nv, d, 0), _forward_difference(nu, nv, d, 1)
+    Bu, Bv = -Du.T.tocsr(), -Dv.T.tocsr()
+    P = sp.bmat([[k * k * e + e @ Dv @ ie @ Bv + Bu @ Du, Bu @ Dv - e @ Dv @ ie @ Bu],
+                 [Bv @ Du - e @ Du @ ie @ Bv, k * k * e + Bv @ Dv + e @ Du @ ie @ Bu]],
+                format="csc")
+    n_top = math.sqrt(float(eps.max())) if n_guess is None else n_guess
+    vals, vecs = spla.eigs(P, k=4, sigma=(k * n_top) ** 2, which="LM")
+    best = None
+    n = nu * nv
+    for val, vec in zip(vals, vecs.T):
+        bt2 = float(np.real(val))
+        if bt2 <= 0 or abs(np.imag(val)) > 1e-6 * abs(bt2):
+            continue
+        hu, hv = vec[:n], vec[n:]
+        # TE-like: horizontal E (Eu ~ beta Hv, Ev ~ -beta Hu) dominates
+        vertical, other = (hv, hu) if horizontal == 0 else (hu, hv)
+        te = np.sum(np.abs(vertical) ** 2) > np.sum(np.abs(other) ** 2)
+        if te and (best is None or bt2 > best[0]):
+            best = (bt2, vec)
+    if best is None:
+        raise ValueError("No guided TE-like mode found")
+    bt2, vec = best
+    vec = vec / vec[np.argmax(np.abs(vec))]
+    bt = math.sqrt(bt2)
+    hu, hv = np.real(vec[:n]), np.real(vec[n:])
+    hw = (Du @ hu + Dv @ hv) / (1j * bt)
+    ew = (Bu @ hv - Bv @ hu) / (1j * k * eps.ravel())
+    eu = (Bv @ hw + 1j * bt * hv) / (1j * k * eps.ravel())
+    ev = (-1j * bt * hu - Bu @ hw) / (1j * k * eps.ravel())
+    beta = 2 / d * math.asin(min(1.0, bt * d / 2))
+    shape = (nu, nv)
+    E = np.stack([eu.reshape(shape), ev.reshape(shape), ew.reshape(shape)])
+    H = np.stack([hu.reshape(shape).astype(complex), hv.reshape(shape).astype(complex),
+                  hw.reshape(shape)])
+    return beta, E, H
 
 
-def mode_fields(eps_plane, d, wavelength, axis, n_guess=2.6):
-    """E and H (3, nu, nv) of the fundamental TE-like mode on a plane normal to
-    `axis` (0: x, 1: y) propagating in +axis, with the dominant E along the
-    plane's horizontal in-plane axis and H' = eta0 H = n_eff x E.  Normalised
-    so that sum over cells of (E x H)_axis = 2 (unit modal power in the
-    detectors' overlap, detectors.py:203-211)."""
-    n_eff, f = solve_mode(eps_plane, d, wavelength, n_guess)
-    E = np.zeros((3,) + f.shape)
-    H = np.zeros((3,) + f.shape)
-    if axis == 0:   # plane (y, z); E_y dominant, H_z = n_eff E_y  -> (E x H)_x = Ey Hz
-        E[1] = f
-        H[2] = n_eff * f
-    else:           # plane (x, z); E_x dominant, H_z = -n_eff E_x -> (E x H)_y = -Ex Hz
-        E[0] = f
-        H[2] = -n_eff * f
-    s = np.sum(np.cross(E, H, axis=0)[axis])
-    scale = math.sqrt(2.0 / s)
-    return n_eff, (E * scale).astype(np.float32), (H * scale).astype(np.float32)
+def _to_global(local, axis):
+    """(3, nu, nv) local-component plane arrays -> global components on the
+    plane's (a, b) index order: axis 0: (u, v, w) = (y, z, x), plane (y, z);
+    axis 1: (u, v, w) = (z, x, y), plane (x, z)."""
+    if axis == 0:
+        return np.stack([local[2], local[0], local[1]])
+    return np.stack([local[1].T, local[2].T, local[0].T])
+
+
+def _colocated(E, H, axis, beta, d, omega, dt):
+    """The detectors' colocation (detectors.py:27-62) applied to the mode:
+    E and H (3, a, b) global-component profiles of the plane, each the
+    amplitude at its own Yee position w_c (the field there being profile *
+    exp(-i beta w_c)), averaged onto the common point of each cell the way the
+    recorder averages the grid, with H's two time levels averaged
+    (cos(w dt / 2)).  Returns the (3, a, b) colocated E and H, phases
+    relative to exp(-i beta w) at the plane itself."""
+    # components half a cell further along the propagation axis: E_w, H_u, H_v
+    half_e = [c == axis for c in range(3)]
+    half_h = [c != axis for c in range(3)]
+
+    def at(F, half, c, sx=0, sy=0, sz=0):
+        """Component c of F at (x + sx, y + sy, z + sz), sx, sy in {-1, 0},
+        sz in {0, 1}, zero outside the plane."""
+        sw = sx if axis == 0 else sy  # cells back along the propagation axis
+        G = F[c] * np.exp(-1j * beta * d * (sw + 0.5 * half[c]))
+        if (sy if axis == 0 else sx):  # one cell back along the plane's first axis
+            G = np.concatenate([np.zeros_like(G[:1]), G[:-1]], axis=0)
+        if sz:
+            G = np.concatenate([G[:, 1:], np.zeros_like(G[:, :1])], axis=1)
+        return G
+
+    def mean(F, half, c, shifts):
+        return sum(at(F, half, c, *sh) for sh in shifts) / len(shifts)
+
+    ec = np.stack([
+        mean(E, half_e, 0, [(0, 0, 0), (-1, 0, 0), (0, 0, 1), (-1, 0, 1)]),
+        mean(E, half_e, 1, [(0, 0, 0), (0, -1, 0), (0, 0, 1), (0, -1, 1)]),
+        at(E, half_e, 2),
+    ])
+    hc = np.stack([
+        mean(H, half_h, 0, [(0, 0, 0), (0, -1, 0)]),
+        mean(H, half_h, 1, [(0, 0, 0), (-1, 0, 0)]),
+        mean(H, half_h, 2, [(sx, sy, sz) for sx in (0, -1) for sy in (0, -1) for sz in (0, 1)]),
+    ]) * math.cos(omega * dt / 2)
+    return ec, hc
+
+
+def mode_fields(eps_plane, d, dt, wavelength, axis):
+    """The Yee-grid TE0 mode (yee_mode) on a plane normal to `axis` (0: x,
+    plane eps[y, z]; 1: y, plane eps[x, z]) propagating in +axis.
+
+    Returns (n_eff, source, detector): `source` = (E, H) float32 (3, a, b),
+    the real transverse components at their Yee positions (longitudinal
+    components zero: the plane source injects only the transverse ones);
+    `detector` = (E, H) complex64, the mode as the recorder sees it after
+    colocation.  Both normalised so that the colocated sum over cells of
+    Re(E x H*)_axis = 2 (unit modal power in the detectors' overlap,
+    detectors.py:203-211)."""
+    local = eps_plane if axis == 0 else eps_plane.T
+    beta, El, Hl = yee_mode(local, d, dt, wavelength, horizontal=0 if axis == 0 else 1)
+    E, H = _to_global(El, axis), _to_global(Hl, axis)
+    omega = 2 * math.pi * C0 / wavelength
+    Ec, Hc = _colocated(E, H, axis, beta, d, omega, dt)
+    power = float(np.sum(np.real(np.cross(Ec, Hc.conj(), axis=0)[axis])))
+    if not power > 0:
+        raise ValueError("Mode solve gave no forward power")
+    scale = math.sqrt(2.0 / power)
+    tr = [c for c in range(3) if c != axis]
+    src_E = np.zeros(E.shape, np.float32)
+    src_H = np.zeros(H.shape, np.float32)
+    src_E[tr] = np.real(E[tr]) * scale
+    src_H[tr] = np.real(H[tr]) * scale
+    return beta * C0 / omega, (src_E, src_H), ((Ec * scale).astype(np.complex64),
+                                               (Hc * scale).astype(np.complex64))
 
 
 # ---------------------------------------------------------------- geometry
@@ -177,7 +300,9 @@ def _detector_schedule(steps):
 def write_scene(path, core, dx, pml, steps, source_x, frequency_hz, pulse, detectors,
                 wavelengths, settings):
     """Assemble and write a bundle.  `detectors` lists (name, axis, position)
-    mode planes; `pulse` is the source object's temporal-profile fields."""
+    mode planes, or (name, axis, position, "-") for the backward-travelling
+    mode (its transverse H negated: the reflected power); `pulse` is the
+    source object's temporal-profile fields."""
     shape = core.shape
     nx, ny, nz = shape
     dt = 0.99 / math.sqrt(3) * dx / C0
@@ -189,7 +314,7 @@ def write_scene(path, core, dx, pml, steps, source_x, frequency_hz, pulse, detec
     objects = []
     add_cpml(arrays, objects, shape, pml, dt, dx, frequency_hz)
     lam0 = C0 / frequency_hz
-    n_eff, Em, Hm = mode_fields(eps[source_x], dx, lam0, 0)
+    n_eff, (Em, Hm), _ = mode_fields(eps[source_x], dx, dt, lam0, 0)
     arrays["source/_E"] = Em[:, None]
     arrays["source/_H"] = Hm[:, None]
     arrays["source/_neff"] = np.array(n_eff, np.complex64)
@@ -209,13 +334,22 @@ def write_scene(path, core, dx, pml, steps, source_x, frequency_hz, pulse, detec
                         phase_shift=0.0, profile_phase_shift=0.0, **pulse))
     freqs = [C0 / w for w in wavelengths]
     idx, window = _detector_schedule(steps)
-    for name, axis, pos in detectors:
+    for name, axis, pos, *way in detectors:
+        direction = way[0] if way else "+"
         sl = [[0, nx], [0, ny], [0, nz]]
         sl[axis] = [pos, pos + 1]
         plane_eps = eps[pos] if axis == 0 else eps[:, pos]
         me, mh = [], []
         for w in wavelengths:
-            _, E, H = mode_fields(plane_eps, dx, w, axis)
+            _, _, (E, H) = mode_fields(plane_eps, dx, dt, w, axis)
+            if direction == "-":  # backward mode: transverse H and longitudinal E flip
+                H = H.copy()
+                E = E.copy()
+                for c in range(3):
+                    if c == axis:
+                        E[c] = -E[c]
+                    else:
+                        H[c] = -H[c]
             me.append(np.expand_dims(E, axis + 1))
             mh.append(np.expand_dims(H, axis + 1))
         arrays[f"{name}/_mode_E"] = np.stack(me).astype(np.complex64)
@@ -223,7 +357,7 @@ def write_scene(path, core, dx, pml, steps, source_x, frequency_hz, pulse, detec
         arrays[f"{name}/_time_step_to_arr_idx"] = idx
         arrays[f"{name}/_window_at_time_step_arr"] = window
         objects.append(dict(name=name, **{"class": "ModeOverlapDetector"}, grid_slice=sl,
-                            direction="+", propagation_axis=axis, mode_index=0,
+                            direction=direction, propagation_axis=axis, mode_index=0,
                             window_sum=float(window.sum()), frequencies_hz=freqs))
     meta = {"settings": dict(spacing_nm=dx * 1e9, precision="float32",
                              exact_interpolation=True, pml_cells=pml, **settings),
@@ -246,16 +380,21 @@ def straight_case(path, spacing_nm=50.0, interior_um=(4.0, 3.0, 2.0), pml=10, st
     pulse = dict(temporal_profile="GaussianPulseProfile", pulse_sigma_s=sigma_t,
                  pulse_delay_s=4 * sigma_t)
     sx = pml + 3
-    dets = [("mode_in", 0, sx + 2), ("mode_out", 0, shape[0] - pml - 3)]
+    dets = [("mode_in", 0, sx + 2), ("mode_reflected", 0, sx + 2, "-"),
+            ("mode_out", 0, shape[0] - pml - 3)]
     return write_scene(path, np.ascontiguousarray(core), dx, pml, steps, sx, f0, pulse, dets,
                        [w * 1e-6 for w in wavelengths_um],
                        dict(scene="straight", domain_um=list(interior_um)))
 
 
 def bend_case(path, spacing_nm=20.0, interior_um=(6.0, 6.0, 2.4), pml=12, steps=4000,
-              radius_um=2.0, nwav=5, width_nm=500.0, height_nm=220.0, pulse_width_fs=100.0):
-    """90-degree Si bend (radius 2 um, 500 x 220 nm) in SiO2, Hann-enveloped pulse
-    at 1.55 um, modal input/output detectors at `nwav` wavelengths in 1.50-1.60 um."""
+              radius_um=2.0, nwav=5, width_nm=500.0, height_nm=220.0, pulse_width_fs=200.0):
+    """90-degree Si bend (radius 2 um, 500 x 220 nm) in SiO2, Hann-windowed
+    pulse (200 fs full width by default) at 1.55 um, modal input (forward and
+    backward) and output detectors at `nwav` wavelengths in 1.50-1.60 um.
+    At 20 nm, 4000 steps are 152 fs of light: the pulse is still being
+    emitted when the run ends, so the transmission is not a converged
+    device figure; the workload is the fixed step count."""
     dx = spacing_nm * 1e-9
     inner = [int(round(v * 1e-6 / dx)) for v in interior_um]
     shape = tuple(n + 2 * pml for n in inner)
@@ -269,7 +408,8 @@ def bend_case(path, spacing_nm=20.0, interior_um=(6.0, 6.0, 2.4), pml=12, steps=
                  pulse_delay_s=width / 2)
     sx = pml + 3
     x_out_guide = pml + int(round((x_turn + R) / dx))
-    dets = [("mode_in", 0, sx + 3), ("mode_out", 1, shape[1] - pml - 4)]
+    dets = [("mode_in", 0, sx + 3), ("mode_reflected", 0, sx + 3, "-"),
+            ("mode_out", 1, shape[1] - pml - 4)]
     del x_out_guide
     return write_scene(path, np.ascontiguousarray(core), dx, pml, steps, sx, f0, pulse, dets,
                        list(np.linspace(1.50e-6, 1.60e-6, nwav)),
