@@ -193,21 +193,40 @@ def reduce_sum(value, world):
     return _reduce(value, world, dist.ReduceOp.SUM) if world > 1 else value
 
 
-def cpu_sample(case, time_steps, threads=None):
-    """The CPU oracle's fused update on the full grid for `time_steps` steps."""
+def cpu_sample(case, time_steps, warmup_steps=0):
+    """The CPU oracle's fused update on the full grid: `warmup_steps` untimed
+    steps (first touch of the field pages), then `time_steps` timed ones, in
+    this process; returns (Gcell-updates/s, threads, seconds)."""
     from oracle import cpu as ocpu
     from oracle.model import OracleSolver
 
     o = OracleSolver(case)
     L = ocpu.lib()
     nx, ny, nz = o.shape
+
+    def run(step0, count):
+        L.oracle_run_steps(o.E, o.H, o.eps, o.psi_e, o.psi_h, o.coeffs["E"], o.coeffs["H"],
+                           o.coeffs["E"].shape[1], o.sources["E"], o.sources["H"], o.waves["E"],
+                           o.waves["H"], o.steps, step0, count, nx, ny, nz, int(o.source_x),
+                           float(o.courant))
+
+    run(0, warmup_steps)
     start = time.perf_counter()
-    L.oracle_run_steps(o.E, o.H, o.eps, o.psi_e, o.psi_h, o.coeffs["E"], o.coeffs["H"],
-                       o.coeffs["E"].shape[1], o.sources["E"], o.sources["H"], o.waves["E"],
-                       o.waves["H"], o.steps, 0, time_steps, nx, ny, nz, int(o.source_x),
-                       float(o.courant))
+    run(warmup_steps, time_steps)
     sec = time.perf_counter() - start
     return o.n * time_steps / sec / 1e9, ocpu.num_threads(), sec
+
+
+def cpu_sample_fresh(case, time_steps, warmup_steps=2):
+    """cpu_sample in a fresh Python process (no torch, no CUDA context, no
+    other thread pool in it): both bench arms time the CPU path this way, so
+    their figures agree."""
+    code = ("import json, sys; sys.path.insert(0, sys.argv[1]); import bench; "
+            "print(json.dumps(bench.cpu_sample(sys.argv[2], int(sys.argv[3]), int(sys.argv[4]))))")
+    out = subprocess.run([sys.executable, "-c", code, str(ROOT), str(case), str(time_steps),
+                          str(warmup_steps)], check=True, capture_output=True, text=True)
+    rate, cores, sec = json.loads(out.stdout.strip().splitlines()[-1])
+    return rate, cores, sec
 
 
 def run_reference(args, world, rank):
@@ -215,17 +234,18 @@ def run_reference(args, world, rank):
     if rank != 0:
         return
     case = make_bundle(args.workload, args.time_steps)
-    sample_steps = int(os.environ.get("FDTD_REF_SAMPLE_STEPS", "20"))
+    sample_steps = args.cpu_steps
     for _ in range(args.warmup):
-        cpu_sample(case, sample_steps)
+        cpu_sample_fresh(case, min(sample_steps, 10))
     rates, secs, cores = [], [], 1
     for _ in range(args.steps):
-        r, cores, s = cpu_sample(case, sample_steps)
+        r, cores, s = cpu_sample_fresh(case, sample_steps)
         rates.append(r)
         secs.append(s)
     value = statistics.median(rates)
-    sample = (f"{sample_steps} of 4000 time steps on the full 324x324x144 grid per step, "
-              "E+H updates with CPML and source (oracle/fdtd_oracle.c, OpenMP)")
+    sample = (f"{sample_steps} of 4000 time steps on the full 324x324x144 grid per step "
+              f"({statistics.median(secs):.1f} s), E+H updates with CPML and source "
+              "(oracle/fdtd_oracle.c, OpenMP), each in a fresh process after 2 untimed steps")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Gcell-updates/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -350,11 +370,15 @@ def run_ours(args, world, rank, local):
     kernel_ms = k0.elapsed_time(k1) / nk
     achieved = BYTES_PER_CELL * s.n * updates / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = load_peaks()
+    # DRAM bytes of one launch of this kernel on this grid, from an ncu
+    # capture of the benchmark itself (null for any other kernel or grid)
     traffic = None
-    tfile = ROOT / "profiles" / "fused_step_traffic.json"
-    if tfile.exists() and args.workload == "bend20":  # the file holds the full bend's figure
+    tfile = ROOT / "profiles" / "block_step_bend20_traffic.json"
+    if tfile.exists() and args.workload == "bend20" and s.time_block == 2:
         try:
-            traffic = json.loads(tfile.read_text()).get("bytes_per_launch")
+            rec = json.loads(tfile.read_text())
+            if rec.get("grid") == list(s.shape) and rec.get("cell_updates_per_launch") == 2:
+                traffic = rec.get("bytes_per_launch")
         except (ValueError, OSError):
             traffic = None
 
@@ -383,11 +407,11 @@ def run_ours(args, world, rank, local):
 
     cpu = None
     if rank == 0 and world == 1 and not args.skip_cpu:
-        sample_steps = int(os.environ.get("FDTD_CPU_SAMPLE_STEPS", "60"))
-        rate, cores, sec = cpu_sample(case, sample_steps)
+        rate, cores, sec = cpu_sample_fresh(case, args.cpu_steps)
         cpu = {"value": rate, "unit": "Gcell-updates/s", "cores": cores, "kind": "port",
-               "sample": f"{sample_steps} of 4000 time steps on the full 324x324x144 grid "
-                         f"({sec:.1f} s), CPU oracle E+H updates with CPML and source"}
+               "sample": f"{args.cpu_steps} of 4000 time steps on the full 324x324x144 grid "
+                         f"({sec:.1f} s, after 2 untimed steps), CPU oracle E+H updates with "
+                         "CPML and source, in a fresh process"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
@@ -398,7 +422,9 @@ def run_ours(args, world, rank, local):
                        else f"{args.workload}_{list(s.shape)}_{s.steps}steps",
                        "grid": list(s.shape), "time_steps": s.steps,
                        "cells": s.n, "materials": "uint8 index (SiO2 2.085, Si 12.11)",
-                       "detectors": "mode_in, mode_out x 5 wavelengths (float64 DFT)",
+                       "detectors": "mode_in (read forward and backward), mode_out x 5 "
+                                    "wavelengths (float64 DFT)",
+                       "pulse": "Hann, 200 fs, 1.55 um",
                        "l2": "inputs larger than L2 (fields 4 x 181 MB ping-pong)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -426,6 +452,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the CPU baseline sample")
+    ap.add_argument("--cpu-steps", type=int, default=20,
+                    help="time steps of the CPU sample (both arms; 4000 = the whole trajectory)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="bend20",
                     help="bend20 is the benchmark; bend20-small is for profiling captures")
     ap.add_argument("--time-steps", type=int, default=None,

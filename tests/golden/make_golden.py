@@ -17,7 +17,7 @@ tests need:
   (results/warp/gradient20/gradient.npz) and its result.json.
 
 Bundles are copied byte for byte so their manifest SHA-256 still matches.
-Run from anywhere:  python tests/golden/make_golden.py [/path/to/reference]
+Run from anywhere:  python tests/golden/make_golden.py /path/to/warp-fdtd
 """
 
 import json
@@ -77,4 +77,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <warp-fdtd checkout>")
+    main(sys.argv[1])
