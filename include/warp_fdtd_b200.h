@@ -337,7 +337,13 @@ int fdtd_batch_release(fdtd_batch_plan *plan);
  * and can write E(n+1) and H(n+1/2) of the cells inside up to
  * FDTD_SNAP_BOXES_MAX boxes (x0, x1, y0, y1, z0, z1, half-open; whole groups
  * of four z cells) to snap_e / snap_h ((3, nx*ny*pitch_z) each), so that
- * detectors can sample the intermediate step. */
+ * detectors can sample the intermediate step.  Blocks below
+ * extra->interior_blocks run a build of the kernel without the x/y CPML
+ * code (schedule them on the grid's CPML-free interior).  args->error, when
+ * set, receives 1 (a bounded wait expired), 2 (z CPML ranks not in groups of
+ * four), 3 (a schedule entry outside the grid or longer than chunk_x) or 4
+ * (an interior block's segment touches x/y CPML); the fields are then not
+ * valid. */
 #define FDTD_BLOCK_GROUPS_MAX 64
 #define FDTD_SNAP_BOXES_MAX 8
 typedef struct fdtd_block_plan {
@@ -357,6 +363,9 @@ typedef struct fdtd_block_extra {
                       b*segments .. b*segments+segments-1 in order, tile < 0 ends the list */
     int nsnap;
     int snap_box[FDTD_SNAP_BOXES_MAX][6];
+    int interior_blocks; /* blocks [0, interior_blocks) run a build without x/y CPML code:
+                            their segments (rows and planes xa-depth-1 .. xb+depth) must
+                            carry no x/y CPML state and 1/kappa == 1, else error 4 */
 } fdtd_block_extra;
 
 int fdtd_step_block_prepare(const fdtd_step_args *args, int depth, fdtd_block_plan *plan);

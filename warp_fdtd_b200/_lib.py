@@ -99,7 +99,8 @@ class BlockExtra(ctypes.Structure):
     """Mirror of `fdtd_block_extra`."""
 
     _fields_ = [("scratch", _p), ("scratch_bytes", _ll), ("snap_e", _p), ("snap_h", _p),
-                ("segments", _i), ("nsnap", _i), ("snap_box", (_i * 6) * SNAP_BOXES_MAX)]
+                ("segments", _i), ("nsnap", _i), ("snap_box", (_i * 6) * SNAP_BOXES_MAX),
+                ("interior_blocks", _i)]
 
 
 class InjectPlane(ctypes.Structure):

@@ -66,6 +66,7 @@ struct Params {
     long long scratch_block;     // floats per block
     float *snap_e, *snap_h;      // D = 2: E(n+1), H(n+1/2) inside the boxes
     int segments;                // schedule entries per block
+    int interior_blocks;         // blocks [0, interior_blocks) run the build without x/y CPML
     int nsnap;
     int snap[FDTD_SNAP_BOXES_MAX][6];
 };
@@ -316,9 +317,8 @@ __device__ __forceinline__ VF<V> h_comb(const VF<V> &o, const VF<V> &u, const VF
     return r;
 }
 
-// Out-of-line pieces of the march.  They run only in CPML slabs, on the
-// source plane or inside snapshot boxes; keeping them out of the loop keeps
-// the loop's instructions within the instruction cache.
+// Pieces of the march that run only in CPML slabs, on the source plane or
+// inside snapshot boxes.
 struct Pair {
     VF<4> a, b;
 };
@@ -326,7 +326,7 @@ struct Pair {
 // One axis's pair of differences with a coefficient uniform over the group and
 // a != 0 (kernels.py:29-47): old state at src / src + sslot, new state to
 // dst / dst + dslot unless dst is null.
-__device__ __noinline__ Pair axis_cpml(Pair d, float4 c, const float *src, long long sslot,
+__device__ __forceinline__ Pair axis_cpml(Pair d, float4 c, const float *src, long long sslot,
                                        float *dst, long long dslot) {
     const VF<4> p0 = ldv<4>(src), p1 = ldv<4>(src + sslot);
     VF<4> n0, n1;
@@ -442,7 +442,7 @@ struct Smem {
 // The march of one thread over the block's segments: V cells per thread,
 // SLAB for the groups with z CPML.  Every thread of the block runs the same
 // sequence of barriers whatever its V.
-template <int MAT, int D, int V, class G>
+template <int MAT, int D, int V, class G, bool XY>
 __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const Smem &sm, int r,
                                       int zv, bool live, bool slab, int rbe, int rbh, bool zEp,
                                       bool zHp, const float4 *zce, const float4 *zch) {
@@ -565,6 +565,18 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
             sm.chy[j] = in ? __ldg(ch + clen + yy) : ident;
         }
         __syncthreads();
+        if constexpr (!XY) {
+            // this build has no x/y CPML code: the segment's rows and every
+            // plane it touches (xa - D - 1 .. xb + D) must have none
+            bool bad = false;
+            for (int j = tid; j < R; j += nth) bad |= active(sm.cey[j]) || active(sm.chy[j]);
+            for (int j = xa - D - 1 + tid; j <= xb + D; j += nth)
+                if (j >= 0 && j < nx) bad |= active(__ldg(ce + j)) || active(__ldg(ch + j));
+            if (__syncthreads_or(bad)) {
+                if (tid == 0 && a.error) atomicExch(a.error, 4);
+                break;
+            }
+        }
         y = yf + r;
         row_in = live && y >= 0 && y < ny;
         own_row = row_in && r >= D - 1 && r < D - 1 + TY;
@@ -624,10 +636,10 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
             const int p = xa - D + k;
             const int q = p - 1, pe = p - 1, ph = p - 2;
             // plane-uniform x coefficients of the updates, in flight during the wait
-            const float4 cxa = p >= 0 && p < nx ? __ldg(ce + p) : ident;
-            const float4 cxb = q >= 0 && q < nx ? __ldg(ch + q) : ident;
-            const float4 cxc = D == 2 && pe >= 0 && pe < nx ? __ldg(ce + pe) : ident;
-            const float4 cxd = D == 2 && ph >= 0 && ph < nx ? __ldg(ch + ph) : ident;
+            const float4 cxa = XY && p >= 0 && p < nx ? __ldg(ce + p) : ident;
+            const float4 cxb = XY && q >= 0 && q < nx ? __ldg(ch + q) : ident;
+            const float4 cxc = XY && D == 2 && pe >= 0 && pe < nx ? __ldg(ce + pe) : ident;
+            const float4 cxd = XY && D == 2 && ph >= 0 && ph < nx ? __ldg(ch + ph) : ident;
             if (++slot == S) {
                 slot = 0;
                 phase ^= 1;
@@ -669,15 +681,15 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 Diff<V> d = e_diffs<V>(Hb + ho, HS, HB, hcur, h0c);
                 const float4 cx = cxa;
                 const bool own = D == 1 && own_row && p >= xa && p < xb;
-                if (cx.x != 0.0f) {
+                if (XY && cx.x != 0.0f) {
                     const i64 ib = prm.xoff + ((i64)(int)cx.w * ny + y) * P + zv;
                     const Pair f = axis_cpml({d.x2, d.x1}, cx, pe_o + ib, xslot, D == 2 ? scr + (i64)((k & 1) * 2 + 0) * 4 * sc_comp : own ? pe_n + ib : nullptr, D == 2 ? sc_comp : xslot);
                     d.x2 = f.a;
                     d.x1 = f.b;
-                } else if (cx.z != 1.0f) {
+                } else if (XY && cx.z != 1.0f) {
                     scale_u<V>(d.x2, d.x1, cx.z);
                 }
-                if (yE) {
+                if (XY && yE) {
                     if (cye.x != 0.0f) {
                         const i64 ib = prm.yoff + ((i64)(int)cye.w * nx + p) * P + zv;
                         const Pair f = axis_cpml({d.y0, d.y2}, cye, pe_o + ib, yslot, D == 2 ? scr + (i64)((k & 1) * 2 + 0) * 4 * sc_comp + 2 * sc_comp : own ? pe_n + ib : nullptr, D == 2 ? sc_comp : yslot);
@@ -722,15 +734,15 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 Diff<V> d = h_diffs<V>(e1p + eo, ES, RW, eq, e1);
                 const float4 cx = cxb;
                 const bool own = D == 1 && own_row && q >= xa && q < xb;
-                if (cx.x != 0.0f) {
+                if (XY && cx.x != 0.0f) {
                     const i64 ib = prm.xoff + ((i64)(int)cx.w * ny + y) * P + zv;
                     const Pair f = axis_cpml({d.x2, d.x1}, cx, ph_o + ib, xslot, D == 2 ? scr + (i64)((k & 1) * 2 + 1) * 4 * sc_comp : own ? ph_n + ib : nullptr, D == 2 ? sc_comp : xslot);
                     d.x2 = f.a;
                     d.x1 = f.b;
-                } else if (cx.z != 1.0f) {
+                } else if (XY && cx.z != 1.0f) {
                     scale_u<V>(d.x2, d.x1, cx.z);
                 }
-                if (yH) {
+                if (XY && yH) {
                     if (cyh.x != 0.0f) {
                         const i64 ib = prm.yoff + ((i64)(int)cyh.w * nx + q) * P + zv;
                         const Pair f = axis_cpml({d.y0, d.y2}, cyh, ph_o + ib, yslot, D == 2 ? scr + (i64)((k & 1) * 2 + 1) * 4 * sc_comp + 2 * sc_comp : own ? ph_n + ib : nullptr, D == 2 ? sc_comp : yslot);
@@ -783,15 +795,15 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                     const int sl = (k - 1) & 1;
                     const float4 cx = cxc;
                     const bool own = own_row && pe >= xa && pe < xb;
-                    if (cx.x != 0.0f) {
+                    if (XY && cx.x != 0.0f) {
                         const i64 ib = prm.xoff + ((i64)(int)cx.w * ny + y) * P + zv;
                         const Pair f = axis_cpml({d.x2, d.x1}, cx, scr + (i64)(sl * 2 + 0) * 4 * sc_comp, sc_comp, own ? pe_n + ib : nullptr, xslot);
                         d.x2 = f.a;
                         d.x1 = f.b;
-                    } else if (cx.z != 1.0f) {
+                    } else if (XY && cx.z != 1.0f) {
                         scale_u<V>(d.x2, d.x1, cx.z);
                     }
-                    if (yE) {
+                    if (XY && yE) {
                         if (cye.x != 0.0f) {
                             const i64 ib = prm.yoff + ((i64)(int)cye.w * nx + pe) * P + zv;
                             const Pair f = axis_cpml({d.y0, d.y2}, cye, scr + (i64)(sl * 2 + 0) * 4 * sc_comp + 2 * sc_comp, sc_comp, own ? pe_n + ib : nullptr, yslot);
@@ -831,15 +843,15 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                     const int sl = (k - 1) & 1;
                     const float4 cx = cxd;
                     const bool own = own_row;
-                    if (cx.x != 0.0f) {
+                    if (XY && cx.x != 0.0f) {
                         const i64 ib = prm.xoff + ((i64)(int)cx.w * ny + y) * P + zv;
                         const Pair f = axis_cpml({d.x2, d.x1}, cx, scr + (i64)(sl * 2 + 1) * 4 * sc_comp, sc_comp, own ? ph_n + ib : nullptr, xslot);
                         d.x2 = f.a;
                         d.x1 = f.b;
-                    } else if (cx.z != 1.0f) {
+                    } else if (XY && cx.z != 1.0f) {
                         scale_u<V>(d.x2, d.x1, cx.z);
                     }
-                    if (yH) {
+                    if (XY && yH) {
                         if (cyh.x != 0.0f) {
                             const i64 ib = prm.yoff + ((i64)(int)cyh.w * nx + ph) * P + zv;
                             const Pair f = axis_cpml({d.y0, d.y2}, cyh, scr + (i64)(sl * 2 + 1) * 4 * sc_comp + 2 * sc_comp, sc_comp, own ? ph_n + ib : nullptr, yslot);
@@ -981,8 +993,15 @@ __global__ void __launch_bounds__(NT, MINB)
         zHp |= zch[j].x != 0.0f;
     }
     const int rbe = slab ? (int)sm.cez[zv].w : 0, rbh = slab ? (int)sm.chz[zv].w : 0;
-    march<MAT, D, 4, G>(maps, prm, sm, live ? r : R - 1, zv, live, slab, rbe, rbh, zEp, zHp, zce,
-                        zch);
+    // blocks scheduled on planes and rows free of x/y CPML run the build
+    // without that code: its call sites and state would otherwise occupy
+    // registers on every iteration
+    if ((int)blockIdx.x < prm.interior_blocks)
+        march<MAT, D, 4, G, false>(maps, prm, sm, live ? r : R - 1, zv, live, slab, rbe, rbh, zEp,
+                                   zHp, zce, zch);
+    else
+        march<MAT, D, 4, G, true>(maps, prm, sm, live ? r : R - 1, zv, live, slab, rbe, rbh, zEp,
+                                  zHp, zce, zch);
 }
 
 using Kernel = void (*)(Maps, Params);
@@ -1228,6 +1247,11 @@ extern "C" int fdtd_step_block(const fdtd_step_args *args, const fdtd_block_plan
     prm.ns = ns;
     prm.ts = (ns * L.R + 31) / 32 * 32;
     prm.segments = extra && extra->segments > 0 ? extra->segments : 1;
+    prm.interior_blocks = extra ? extra->interior_blocks : 0;
+    if (prm.interior_blocks < 0 || prm.interior_blocks > blocks) {
+        set_error("fdtd_step_block: interior_blocks %d outside 0..%d", prm.interior_blocks, blocks);
+        return FDTD_ERR_ARG;
+    }
     if (prm.segments > 1 && !a.schedule) {
         set_error("fdtd_step_block: several segments per block need a schedule");
         return FDTD_ERR_ARG;

@@ -25,8 +25,7 @@ import torch
 
 from . import _lib
 from . import kernels as k
-from .schedule import (BLOCK_SEGMENT_COST, BLOCK_X_WEIGHT, BLOCK_Y_WEIGHT, X_WEIGHT, Y_WEIGHT,
-                       balanced_schedule, segment_schedule)
+from .schedule import X_WEIGHT, Y_WEIGHT, balanced_schedule, split_segment_schedule
 from ._lib import ptr
 from .bundle import read_bundle
 
@@ -625,8 +624,8 @@ class Solver:
             plan = _lib.BlockPlan()
             _lib.call("fdtd_step_block_prepare", ctypes.byref(base), depth, ctypes.byref(plan))
             slots = max(1, plan.blocks_per_sm) * max(1, plan.sms)
-            runs, segments = segment_schedule(self.shape, plan.tile_y, ce, ch, slots,
-                                              BLOCK_Y_WEIGHT, BLOCK_X_WEIGHT, BLOCK_SEGMENT_COST)
+            runs, segments, interior = split_segment_schedule(self.shape, plan.tile_y, depth,
+                                                              ce, ch, slots)
             nblocks = runs.shape[0] // segments
             sched = torch.from_numpy(runs).to(self.device)
             base.tile_y = plan.tile_y
@@ -637,6 +636,7 @@ class Solver:
             pair = [base, self._swapped(base)]
             extra = _lib.BlockExtra()
             extra.segments = int(segments)
+            extra.interior_blocks = int(interior)
             scratch = None
             if depth == 2:
                 nbytes = int(plan.scratch_block_bytes) * int(nblocks)
@@ -687,6 +687,7 @@ class Solver:
             extra.scratch = info["extra"].scratch
             extra.scratch_bytes = info["extra"].scratch_bytes
             extra.segments = info["extra"].segments
+            extra.interior_blocks = info["extra"].interior_blocks
             if boxes:
                 if self._mid is None:
                     f32 = dict(dtype=torch.float32, device=self.device)
