@@ -20,8 +20,8 @@
 // time step at D = 2.
 //
 // Threads: one per group of four consecutive z cells of one row.  Groups whose
-// cells carry z CPML ("slab" groups) are packed into their own warps after the
-// plain groups, so the z filter is a warp-uniform branch: plain warps never
+// cells carry z CPML ("slab" groups) are packed into their own warps before
+// the plain groups, so the z filter is a warp-uniform branch: plain warps never
 // execute it.  x CPML is uniform over a plane, y CPML over a row.
 //
 // CPML state ping-pongs like the fields (slab layout, FDTD_PSI_SLAB): step 1
@@ -223,22 +223,23 @@ __device__ __forceinline__ void scale_u(VF<V> &d0, VF<V> &d1, float k) {
     }
 }
 
-// z axis: a coefficient per cell; inactive cells keep zero state.
+// z axis: a coefficient per cell; inactive cells (a == 0) keep zero state and
+// give d / kappa.  Both results are computed and one is selected: lanes of a
+// warp hold different groups, and a branch per cell would split the warp.
 template <int V>
 __device__ __forceinline__ void filt_z(VF<V> &d0, VF<V> &d1, const float4 *cz, const VF<V> &p0,
                                        const VF<V> &p1, VF<V> &n0, VF<V> &n1) {
 #pragma unroll
     for (int j = 0; j < V; ++j) {
         const float4 c = cz[j];
-        if (c.x != 0.0f) {
-            d0.v[j] = cp1(d0.v[j], c, p0.v[j], n0.v[j]);
-            d1.v[j] = cp1(d1.v[j], c, p1.v[j], n1.v[j]);
-        } else {
-            d0.v[j] = c.z * d0.v[j];
-            d1.v[j] = c.z * d1.v[j];
-            n0.v[j] = 0.0f;
-            n1.v[j] = 0.0f;
-        }
+        const bool on = c.x != 0.0f;
+        const float k0 = c.z * d0.v[j], k1 = c.z * d1.v[j];
+        const float q0 = c.y * p0.v[j] + c.x * d0.v[j];
+        const float q1 = c.y * p1.v[j] + c.x * d1.v[j];
+        d0.v[j] = on ? k0 + q0 : k0;
+        d1.v[j] = on ? k1 + q1 : k1;
+        n0.v[j] = on ? q0 : 0.0f;
+        n1.v[j] = on ? q1 : 0.0f;
     }
 }
 
@@ -319,36 +320,38 @@ __device__ __forceinline__ VF<V> h_comb(const VF<V> &o, const VF<V> &u, const VF
 
 // Pieces of the march that run only in CPML slabs, on the source plane or
 // inside snapshot boxes.
+template <int V>
 struct Pair {
-    VF<4> a, b;
+    VF<V> a, b;
 };
 
 // One axis's pair of differences with a coefficient uniform over the group and
 // a != 0 (kernels.py:29-47): old state at src / src + sslot, new state to
 // dst / dst + dslot unless dst is null.
-__device__ __forceinline__ Pair axis_cpml(Pair d, float4 c, const float *src, long long sslot,
-                                       float *dst, long long dslot) {
-    const VF<4> p0 = ldv<4>(src), p1 = ldv<4>(src + sslot);
-    VF<4> n0, n1;
-    filt_u<4>(d.a, d.b, c, p0, p1, n0, n1);
+template <int V>
+__device__ __forceinline__ Pair<V> axis_cpml(Pair<V> d, float4 c, const float *src, long long sslot,
+                                          float *dst, long long dslot) {
+    const VF<V> p0 = ldv<V>(src), p1 = ldv<V>(src + sslot);
+    VF<V> n0, n1;
+    filt_u<V>(d.a, d.b, c, p0, p1, n0, n1);
     if (dst) {
-        stv<4>(dst, n0);
-        stv<4>(dst + dslot, n1);
+        stv<V>(dst, n0);
+        stv<V>(dst + dslot, n1);
     }
     return d;
 }
 
-// The z pair with per-cell coefficients cz (kept in the slab lane's
-// registers); state at src / src + sslot, new state to dst / dst + dslot
-// unless dst is null, when `has`.
-__device__ __forceinline__ Pair z_cpml(Pair d, const float4 *cz, bool has, const float *src,
-                                       long long sslot, float *dst, long long dslot) {
-    const VF<4> p0 = has ? ldv<4>(src) : zerov<4>(), p1 = has ? ldv<4>(src + sslot) : zerov<4>();
-    VF<4> n0, n1;
-    filt_z<4>(d.a, d.b, cz, p0, p1, n0, n1);
+// The z pair with per-cell coefficients cz (shared memory); state at src /
+// src + sslot, new state to dst / dst + dslot unless dst is null, when `has`.
+template <int V>
+__device__ __forceinline__ Pair<V> z_cpml(Pair<V> d, const float4 *cz, bool has, const float *src,
+                                          long long sslot, float *dst, long long dslot) {
+    const VF<V> p0 = has ? ldv<V>(src) : zerov<V>(), p1 = has ? ldv<V>(src + sslot) : zerov<V>();
+    VF<V> n0, n1;
+    filt_z<V>(d.a, d.b, cz, p0, p1, n0, n1);
     if (has && dst) {
-        stv<4>(dst, n0);
-        stv<4>(dst + dslot, n1);
+        stv<V>(dst, n0);
+        stv<V>(dst + dslot, n1);
     }
     return d;
 }
@@ -356,13 +359,14 @@ __device__ __forceinline__ Pair z_cpml(Pair d, const float4 *cz, bool has, const
 // kernels.py:130-137 (electric, with inverse permittivity) and 138-141
 // (magnetic) plane source at time tw for the group's cells below nz:
 // components 1 and 2 in `v`.
-__device__ __noinline__ Pair plane_source(Pair v, VF<4> ie, bool electric, const float *src,
-                                          const float *waves, long long wc, long long syz, int nz,
-                                          int y, int zv, int tw, float C) {
+template <int V>
+__device__ __noinline__ Pair<V> plane_source(Pair<V> v, VF<V> ie, bool electric, const float *src,
+                                             const float *waves, long long wc, long long syz,
+                                             int nz, int y, int zv, int tw, float C) {
     if (tw < 0 || tw >= wc) return v;
     const float w2 = waves[2 * wc + tw], w1 = waves[wc + tw];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < V; ++j) {
         const int gz = zv + j;
         if (gz < nz) {
             const long long si = (long long)y * nz + gz;
@@ -381,12 +385,13 @@ __device__ __noinline__ Pair plane_source(Pair v, VF<4> ie, bool electric, const
 // Snapshot of the group's three components (inline: the blocks owning a
 // detector row store one every iteration, and one wave waits for its slowest
 // block).
-__device__ __forceinline__ void snap_store(float *base, long long off, long long cols, VF<4> v0,
-                                        VF<4> v1, VF<4> v2) {
+template <int V>
+__device__ __forceinline__ void snap_store(float *base, long long off, long long cols, VF<V> v0,
+                                           VF<V> v1, VF<V> v2) {
     float *dst = base + off;
-    stv<4>(dst, v0);
-    stv<4>(dst + cols, v1);
-    stv<4>(dst + 2 * cols, v2);
+    stv<V>(dst, v0);
+    stv<V>(dst + cols, v1);
+    stv<V>(dst + 2 * cols, v2);
 }
 
 // A slab group must hold the aligned consecutive ranks rb .. rb+3 of its
@@ -683,7 +688,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 const bool own = D == 1 && own_row && p >= xa && p < xb;
                 if (XY && cx.x != 0.0f) {
                     const i64 ib = prm.xoff + ((i64)(int)cx.w * ny + y) * P + zv;
-                    const Pair f = axis_cpml({d.x2, d.x1}, cx, pe_o + ib, xslot, D == 2 ? scr + (i64)((k & 1) * 2 + 0) * 4 * sc_comp : own ? pe_n + ib : nullptr, D == 2 ? sc_comp : xslot);
+                    const Pair<V> f = axis_cpml<V>({d.x2, d.x1}, cx, pe_o + ib, xslot, D == 2 ? scr + (i64)((k & 1) * 2 + 0) * 4 * sc_comp : own ? pe_n + ib : nullptr, D == 2 ? sc_comp : xslot);
                     d.x2 = f.a;
                     d.x1 = f.b;
                 } else if (XY && cx.z != 1.0f) {
@@ -692,7 +697,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 if (XY && yE) {
                     if (cye.x != 0.0f) {
                         const i64 ib = prm.yoff + ((i64)(int)cye.w * nx + p) * P + zv;
-                        const Pair f = axis_cpml({d.y0, d.y2}, cye, pe_o + ib, yslot, D == 2 ? scr + (i64)((k & 1) * 2 + 0) * 4 * sc_comp + 2 * sc_comp : own ? pe_n + ib : nullptr, D == 2 ? sc_comp : yslot);
+                        const Pair<V> f = axis_cpml<V>({d.y0, d.y2}, cye, pe_o + ib, yslot, D == 2 ? scr + (i64)((k & 1) * 2 + 0) * 4 * sc_comp + 2 * sc_comp : own ? pe_n + ib : nullptr, D == 2 ? sc_comp : yslot);
                         d.y0 = f.a;
                         d.y2 = f.b;
                     } else {
@@ -701,7 +706,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 }
                 if (slab) {
                     const i64 ib = prm.zoff + ((i64)p * ny + y) * RZ + rbe;
-                    const Pair f = z_cpml({d.z1, d.z0}, zce, zEp, (const float *)(st + off_pze) + r * RZ + rbe, R * RZ, D == 2 ? sm.zr + ((k & 1) * 2 + 0) * 2 * zr_comp + r * RZ + rbe : own ? pe_n + ib : nullptr, D == 2 ? (i64)zr_comp : zslot);
+                    const Pair<V> f = z_cpml<V>({d.z1, d.z0}, zce, zEp, (const float *)(st + off_pze) + r * RZ + rbe, R * RZ, D == 2 ? sm.zr + ((k & 1) * 2 + 0) * 2 * zr_comp + r * RZ + rbe : own ? pe_n + ib : nullptr, D == 2 ? (i64)zr_comp : zslot);
                     d.z1 = f.a;
                     d.z0 = f.b;
                 }
@@ -711,7 +716,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 e1[1] = e_comb<V>(eo3[1], d.z0, d.x2, C, ie);
                 e1[2] = e_comb<V>(eo3[2], d.x1, d.y0, C, ie);
                 if (p == a.source_x) {
-                    const Pair v = plane_source({e1[1], e1[2]}, ie, true, a.src_h, a.waves_h, wc,
+                    const Pair<V> v = plane_source<V>({e1[1], e1[2]}, ie, true, a.src_h, a.waves_h, wc,
                                                 syz, nz, y, zv, t, C);
                     e1[1] = v.a;
                     e1[2] = v.b;
@@ -720,7 +725,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 if (D == 1) {
                     if (own) store3(En, p, e1);
                 } else if (snap_hit(p)) {
-                    snap_store(prm.snap_e, p * plane + grow, cols, e1[0], e1[1], e1[2]);
+                    snap_store<V>(prm.snap_e, p * plane + grow, cols, e1[0], e1[1], e1[2]);
                 }
             }
             if (live) st3(e1w + eo, ES, e1);
@@ -736,7 +741,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 const bool own = D == 1 && own_row && q >= xa && q < xb;
                 if (XY && cx.x != 0.0f) {
                     const i64 ib = prm.xoff + ((i64)(int)cx.w * ny + y) * P + zv;
-                    const Pair f = axis_cpml({d.x2, d.x1}, cx, ph_o + ib, xslot, D == 2 ? scr + (i64)((k & 1) * 2 + 1) * 4 * sc_comp : own ? ph_n + ib : nullptr, D == 2 ? sc_comp : xslot);
+                    const Pair<V> f = axis_cpml<V>({d.x2, d.x1}, cx, ph_o + ib, xslot, D == 2 ? scr + (i64)((k & 1) * 2 + 1) * 4 * sc_comp : own ? ph_n + ib : nullptr, D == 2 ? sc_comp : xslot);
                     d.x2 = f.a;
                     d.x1 = f.b;
                 } else if (XY && cx.z != 1.0f) {
@@ -745,7 +750,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 if (XY && yH) {
                     if (cyh.x != 0.0f) {
                         const i64 ib = prm.yoff + ((i64)(int)cyh.w * nx + q) * P + zv;
-                        const Pair f = axis_cpml({d.y0, d.y2}, cyh, ph_o + ib, yslot, D == 2 ? scr + (i64)((k & 1) * 2 + 1) * 4 * sc_comp + 2 * sc_comp : own ? ph_n + ib : nullptr, D == 2 ? sc_comp : yslot);
+                        const Pair<V> f = axis_cpml<V>({d.y0, d.y2}, cyh, ph_o + ib, yslot, D == 2 ? scr + (i64)((k & 1) * 2 + 1) * 4 * sc_comp + 2 * sc_comp : own ? ph_n + ib : nullptr, D == 2 ? sc_comp : yslot);
                         d.y0 = f.a;
                         d.y2 = f.b;
                     } else {
@@ -754,7 +759,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 }
                 if (slab) {
                     const i64 ib = prm.zoff + ((i64)q * ny + y) * RZ + rbh;
-                    const Pair f = z_cpml({d.z1, d.z0}, zch, zHp, (const float *)(st + off_pzh) + r * RZ + rbh, R * RZ, D == 2 ? sm.zr + ((k & 1) * 2 + 1) * 2 * zr_comp + r * RZ + rbh : own ? ph_n + ib : nullptr, D == 2 ? (i64)zr_comp : zslot);
+                    const Pair<V> f = z_cpml<V>({d.z1, d.z0}, zch, zHp, (const float *)(st + off_pzh) + r * RZ + rbh, R * RZ, D == 2 ? sm.zr + ((k & 1) * 2 + 1) * 2 * zr_comp + r * RZ + rbh : own ? ph_n + ib : nullptr, D == 2 ? (i64)zr_comp : zslot);
                     d.z1 = f.a;
                     d.z0 = f.b;
                 }
@@ -762,7 +767,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 h1[1] = h_comb<V>(h0c[1], d.z0, d.x2, C);
                 h1[2] = h_comb<V>(h0c[2], d.x1, d.y0, C);
                 if (q == a.source_x) {
-                    const Pair v = plane_source({h1[1], h1[2]}, zerov<V>(), false, a.src_e,
+                    const Pair<V> v = plane_source<V>({h1[1], h1[2]}, zerov<V>(), false, a.src_e,
                                                 a.waves_e, wc, syz, nz, y, zv, t, C);
                     h1[1] = v.a;
                     h1[2] = v.b;
@@ -770,7 +775,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                 if (D == 1) {
                     if (own) store3(Hn, q, h1);
                 } else if (snap_hit(q)) {
-                    snap_store(prm.snap_h, q * plane + grow, cols, h1[0], h1[1], h1[2]);
+                    snap_store<V>(prm.snap_h, q * plane + grow, cols, h1[0], h1[1], h1[2]);
                 }
             }
             if (D == 2 && r < R - 1) st3(h1w + ho, HS, h1);
@@ -797,7 +802,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                     const bool own = own_row && pe >= xa && pe < xb;
                     if (XY && cx.x != 0.0f) {
                         const i64 ib = prm.xoff + ((i64)(int)cx.w * ny + y) * P + zv;
-                        const Pair f = axis_cpml({d.x2, d.x1}, cx, scr + (i64)(sl * 2 + 0) * 4 * sc_comp, sc_comp, own ? pe_n + ib : nullptr, xslot);
+                        const Pair<V> f = axis_cpml<V>({d.x2, d.x1}, cx, scr + (i64)(sl * 2 + 0) * 4 * sc_comp, sc_comp, own ? pe_n + ib : nullptr, xslot);
                         d.x2 = f.a;
                         d.x1 = f.b;
                     } else if (XY && cx.z != 1.0f) {
@@ -806,7 +811,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                     if (XY && yE) {
                         if (cye.x != 0.0f) {
                             const i64 ib = prm.yoff + ((i64)(int)cye.w * nx + pe) * P + zv;
-                            const Pair f = axis_cpml({d.y0, d.y2}, cye, scr + (i64)(sl * 2 + 0) * 4 * sc_comp + 2 * sc_comp, sc_comp, own ? pe_n + ib : nullptr, yslot);
+                            const Pair<V> f = axis_cpml<V>({d.y0, d.y2}, cye, scr + (i64)(sl * 2 + 0) * 4 * sc_comp + 2 * sc_comp, sc_comp, own ? pe_n + ib : nullptr, yslot);
                             d.y0 = f.a;
                             d.y2 = f.b;
                         } else {
@@ -815,7 +820,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                     }
                     if (slab) {
                         const i64 ib = prm.zoff + ((i64)pe * ny + y) * RZ + rbe;
-                        const Pair f = z_cpml({d.z1, d.z0}, zce, zEp, sm.zr + (sl * 2 + 0) * 2 * zr_comp + r * RZ + rbe, zr_comp, own ? pe_n + ib : nullptr, zslot);
+                        const Pair<V> f = z_cpml<V>({d.z1, d.z0}, zce, zEp, sm.zr + (sl * 2 + 0) * 2 * zr_comp + r * RZ + rbe, zr_comp, own ? pe_n + ib : nullptr, zslot);
                         d.z1 = f.a;
                         d.z0 = f.b;
                     }
@@ -825,7 +830,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                     e2[1] = e_comb<V>(eold[1], d.z0, d.x2, C, iep);
                     e2[2] = e_comb<V>(eold[2], d.x1, d.y0, C, iep);
                     if (pe == a.source_x) {
-                        const Pair v = plane_source({e2[1], e2[2]}, iep, true, a.src_h, a.waves_h,
+                        const Pair<V> v = plane_source<V>({e2[1], e2[2]}, iep, true, a.src_h, a.waves_h,
                                                     wc, syz, nz, y, zv, t + 1, C);
                         e2[1] = v.a;
                         e2[2] = v.b;
@@ -845,7 +850,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                     const bool own = own_row;
                     if (XY && cx.x != 0.0f) {
                         const i64 ib = prm.xoff + ((i64)(int)cx.w * ny + y) * P + zv;
-                        const Pair f = axis_cpml({d.x2, d.x1}, cx, scr + (i64)(sl * 2 + 1) * 4 * sc_comp, sc_comp, own ? ph_n + ib : nullptr, xslot);
+                        const Pair<V> f = axis_cpml<V>({d.x2, d.x1}, cx, scr + (i64)(sl * 2 + 1) * 4 * sc_comp, sc_comp, own ? ph_n + ib : nullptr, xslot);
                         d.x2 = f.a;
                         d.x1 = f.b;
                     } else if (XY && cx.z != 1.0f) {
@@ -854,7 +859,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                     if (XY && yH) {
                         if (cyh.x != 0.0f) {
                             const i64 ib = prm.yoff + ((i64)(int)cyh.w * nx + ph) * P + zv;
-                            const Pair f = axis_cpml({d.y0, d.y2}, cyh, scr + (i64)(sl * 2 + 1) * 4 * sc_comp + 2 * sc_comp, sc_comp, own ? ph_n + ib : nullptr, yslot);
+                            const Pair<V> f = axis_cpml<V>({d.y0, d.y2}, cyh, scr + (i64)(sl * 2 + 1) * 4 * sc_comp + 2 * sc_comp, sc_comp, own ? ph_n + ib : nullptr, yslot);
                             d.y0 = f.a;
                             d.y2 = f.b;
                         } else {
@@ -863,7 +868,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                     }
                     if (slab) {
                         const i64 ib = prm.zoff + ((i64)ph * ny + y) * RZ + rbh;
-                        const Pair f = z_cpml({d.z1, d.z0}, zch, zHp, sm.zr + (sl * 2 + 1) * 2 * zr_comp + r * RZ + rbh, zr_comp, own ? ph_n + ib : nullptr, zslot);
+                        const Pair<V> f = z_cpml<V>({d.z1, d.z0}, zch, zHp, sm.zr + (sl * 2 + 1) * 2 * zr_comp + r * RZ + rbh, zr_comp, own ? ph_n + ib : nullptr, zslot);
                         d.z1 = f.a;
                         d.z0 = f.b;
                     }
@@ -872,7 +877,7 @@ __device__ __forceinline__ void march(const Maps &maps, const Params &prm, const
                     h2[1] = h_comb<V>(h1c[1], d.z0, d.x2, C);
                     h2[2] = h_comb<V>(h1c[2], d.x1, d.y0, C);
                     if (ph == a.source_x) {
-                        const Pair v = plane_source({h2[1], h2[2]}, zerov<V>(), false, a.src_e,
+                        const Pair<V> v = plane_source<V>({h2[1], h2[2]}, zerov<V>(), false, a.src_e,
                                                     a.waves_e, wc, syz, nz, y, zv, t + 1, C);
                         h2[1] = v.a;
                         h2[2] = v.b;
@@ -973,35 +978,35 @@ __global__ void __launch_bounds__(NT, MINB)
     // all warps keeps the loop's code small.
     // (slab warps first: they carry the longest dependency chains)
     const bool slab = tid < prm.ts;
-    int r, g;
+    int r, zv;
     if (slab) {
         r = tid / prm.ns;
-        g = prm.group[prm.ni + (tid - r * prm.ns)];
+        zv = 4 * prm.group[prm.ni + (tid - r * prm.ns)];
     } else {
         const int u = tid - prm.ts;
         r = u / prm.ni;
-        g = prm.group[u - r * prm.ni];
+        zv = 4 * prm.group[u - r * prm.ni];
     }
     const bool live = r < R;
-    const int zv = 4 * g;
     bool zEp = false, zHp = false;
-    float4 zce[4], zch[4];
-    for (int j = 0; j < 4; ++j) {
-        zce[j] = slab ? sm.cez[zv + j] : ident;
-        zch[j] = slab ? sm.chz[zv + j] : ident;
-        zEp |= zce[j].x != 0.0f;
-        zHp |= zch[j].x != 0.0f;
-    }
+    if (slab)
+        for (int j = 0; j < 4; ++j) {
+            zEp |= sm.cez[zv + j].x != 0.0f;
+            zHp |= sm.chz[zv + j].x != 0.0f;
+        }
     const int rbe = slab ? (int)sm.cez[zv].w : 0, rbh = slab ? (int)sm.chz[zv].w : 0;
+    // the z coefficients stay in shared memory: registers held for them by
+    // every thread would cost the plain threads more than the loads cost the
+    // slab threads
+    const float4 *zce = sm.cez + zv, *zch = sm.chz + zv;
+    const int rr = live ? r : R - 1;
     // blocks scheduled on planes and rows free of x/y CPML run the build
     // without that code: its call sites and state would otherwise occupy
     // registers on every iteration
     if ((int)blockIdx.x < prm.interior_blocks)
-        march<MAT, D, 4, G, false>(maps, prm, sm, live ? r : R - 1, zv, live, slab, rbe, rbh, zEp,
-                                   zHp, zce, zch);
+        march<MAT, D, 4, G, false>(maps, prm, sm, rr, zv, live, slab, rbe, rbh, zEp, zHp, zce, zch);
     else
-        march<MAT, D, 4, G, true>(maps, prm, sm, live ? r : R - 1, zv, live, slab, rbe, rbh, zEp,
-                                  zHp, zce, zch);
+        march<MAT, D, 4, G, true>(maps, prm, sm, rr, zv, live, slab, rbe, rbh, zEp, zHp, zce, zch);
 }
 
 using Kernel = void (*)(Maps, Params);
@@ -1042,8 +1047,8 @@ static Kernel pick(int mat, int D, int threads, int pair, const Layout &L) {
 constexpr int SMEM_MAX = 227 * 1024;
 constexpr int THREADS_MAX = 512;
 
-// one lane per group of four z cells and row; plain lanes first, slab lanes
-// in warps of their own
+// one lane per group of four z cells and row; the slab lanes (groups with z
+// CPML) in warps of their own
 static int threads_for(int ni, int ns, int R) {
     return (ni * R + 31) / 32 * 32 + (ns * R + 31) / 32 * 32;
 }
