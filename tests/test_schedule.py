@@ -53,3 +53,38 @@ def test_small_grid_caps_runs_at_one_plane():
     for t in range(3):
         mine = runs[runs[:, 0] == t]
         assert mine[0, 1] == 0 and mine[-1, 2] == 13 and np.all(mine[1:, 1] == mine[:-1, 2])
+
+
+def test_split_schedule_keeps_interior_blocks_off_cpml():
+    """The time-blocked kernel's schedule: every (tile, plane) once; the first
+    `interior` blocks only get planes whose whole reach (x0 - depth - 1 ..
+    x1 + depth) and rows carry no x/y CPML, as their build has no CPML code."""
+    from warp_fdtd_b200.schedule import interior_region, split_segment_schedule
+
+    shape, ty, depth = (324, 324, 144), 7, 2
+    ce, ch = _tables(shape, slab=12)
+    runs, M, nin = split_segment_schedule(shape, ty, depth, ce, ch, 148)
+    assert runs.shape == (148 * M, 4) and 0 < nin < 148
+    tiles = (shape[1] + ty - 1) // ty
+    cover = np.zeros((tiles, shape[0]), int)
+    for t, a, b, _ in runs:
+        if t >= 0:
+            cover[t, a:b] += 1
+    assert (cover == 1).all()
+    ok, x0, x1 = interior_region(shape, ty, depth, ce, ch)
+    assert (x0, x1) == (12 + depth + 1, 324 - 12 - depth - 1)
+    rows = ty + 2 * depth - 1
+    xact = (ce[0, :324, 0] != 0) | (ch[0, :324, 0] != 0)
+    yact = (ce[1, :324, 0] != 0) | (ch[1, :324, 0] != 0)
+    for b in range(nin):
+        for t, a, e, _ in runs[b * M:(b + 1) * M]:
+            if t < 0:
+                continue
+            assert not xact[max(0, a - depth - 1):e + depth + 1].any()
+            yf = t * ty - (depth - 1)
+            assert not yact[max(0, yf):yf + rows].any()
+    # without CPML on x and y every block is an interior block
+    for c in (ce, ch):
+        c[:2, :, 0] = 0
+    runs, M, nin = split_segment_schedule(shape, ty, depth, ce, ch, 148)
+    assert nin == 148

@@ -62,6 +62,7 @@ struct Params {
     long long xoff, yoff, zoff;  // slab-block offsets (elements) inside a psi buffer
     int ni, ns, ts;              // plain / slab groups per row, threads of the slab lanes
     unsigned char group[FDTD_BLOCK_GROUPS_MAX];  // z groups: plain ones, then slab ones
+    unsigned char warp_rows[16];  // plain warps: which run of 32 plain lanes each takes
     float *scratch;              // D = 2: per-block x/y CPML ring
     long long scratch_block;     // floats per block
     float *snap_e, *snap_h;      // D = 2: E(n+1), H(n+1/2) inside the boxes
@@ -983,7 +984,7 @@ __global__ void __launch_bounds__(NT, MINB)
         r = tid / prm.ns;
         zv = 4 * prm.group[prm.ni + (tid - r * prm.ns)];
     } else {
-        const int u = tid - prm.ts;
+        const int u = 32 * prm.warp_rows[(tid - prm.ts) >> 5] + (tid & 31);
         r = u / prm.ni;
         zv = 4 * prm.group[u - r * prm.ni];
     }
@@ -1262,6 +1263,39 @@ extern "C" int fdtd_step_block(const fdtd_step_args *args, const fdtd_block_plan
         return FDTD_ERR_ARG;
     }
     for (int j = 0; j < ni + ns; ++j) prm.group[j] = plan->group[j];
+    {
+        // Warps run on the SM's four schedulers by warp index mod 4.  The
+        // slab warps (first) carry the longest work between two barriers, so
+        // the plain warps that share their schedulers get the plain lanes
+        // with the least work: the rows that skip phases (halo rows and the
+        // padding lanes past the last row).
+        const int nplain = (threads_for(ni, ns, L.R) - prm.ts) / 32, sw = prm.ts / 32;
+        int work[16], order[16];
+        for (int w = 0; w < nplain && w < 16; ++w) {
+            work[w] = 0;
+            for (int l = 0; l < 32; ++l) {
+                const int u = 32 * w + l, r = u / ni;
+                if (r >= L.R) continue;
+                int ph = 1 + (r < L.R - 1);
+                if (D == 2) ph += (r >= 1 && r < L.R - 1) + (r >= 1 && r < L.R - 2);
+                work[w] = work[w] > ph ? work[w] : ph;
+            }
+            order[w] = w;
+        }
+        for (int i = 0; i < nplain && i < 16; ++i)  // lightest first
+            for (int j = i + 1; j < nplain && j < 16; ++j)
+                if (work[order[j]] < work[order[i]]) {
+                    const int t = order[i];
+                    order[i] = order[j];
+                    order[j] = t;
+                }
+        bool slab_sched[4] = {false, false, false, false};
+        for (int w = 0; w < sw; ++w) slab_sched[w & 3] = true;
+        int next = 0;
+        for (int pass = 0; pass < 2; ++pass)  // slab schedulers' warps first
+            for (int w = 0; w < nplain && w < 16; ++w)
+                if (slab_sched[(sw + w) & 3] == (pass == 0)) prm.warp_rows[w] = (unsigned char)order[next++];
+    }
     if (D == 2) {
         if (!extra || !extra->scratch || ((uintptr_t)extra->scratch & 15) ||
             extra->scratch_bytes < plan->scratch_block_bytes * blocks) {

@@ -29,16 +29,16 @@ MAX_RUN = 96
 Y_WEIGHT = 0.9
 X_WEIGHT = 0.7
 
-# The same for the time-blocked kernel (fdtd_step_block), and the cost of a
-# block's extra segment in planes: a least-squares fit of per-block durations
-# (globaltimer at block start and end) on the 20 nm bend at depth 2, tile 7.
-BLOCK_Y_WEIGHT = 0.61
-BLOCK_X_WEIGHT = 0.60
-BLOCK_SEGMENT_COST = 2.9
-# A plane run by the time-blocked kernel's interior build (no x/y CPML code)
-# relative to the same plane in the general build (B200, 20 nm bend, depth 2,
-# tile 7: 0.295 vs 0.3645 ms per launch with the CPML switched off in both).
-BLOCK_INTERIOR_COST = 0.81
+# The same for the time-blocked kernel (fdtd_step_block): the extra cost of
+# a y-slab tile plane / an x-slab plane and the cost of a block's extra
+# segment, in planes of the general build, and the cost of a plane run by the
+# interior build (no x/y CPML code).  Least-squares fits of per-block
+# durations (globaltimer at block start and end) on the 20 nm bend at depth
+# 2, tile 7, then the best of a sweep around them (B200).
+BLOCK_Y_WEIGHT = 0.75
+BLOCK_X_WEIGHT = 0.75
+BLOCK_SEGMENT_COST = 3.4
+BLOCK_INTERIOR_COST = 0.78
 
 
 def plane_costs(shape, tile_y, coeff_e, coeff_h, wy=Y_WEIGHT, wx=X_WEIGHT):
