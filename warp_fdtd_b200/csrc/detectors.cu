@@ -234,8 +234,12 @@ __global__ void record_stage_many_kernel(const float *__restrict__ E0, const flo
     stage_block_done(step, done, delta);  // every thread of the block reaches it
 }
 
-// One thread per (component, cell); the window's weights are staged in
-// shared memory ([k][t] float2).
+// One thread per (component, cell) and group of up to FOLD_K frequencies: the
+// thread reads its cell's staged samples once and feeds every frequency of
+// its group; each phasor still sums its steps in time order.  The window's
+// weights are staged in shared memory ([k][t] float2).
+constexpr int FOLD_K = 8;
+
 __global__ void dft_fold_kernel(const int *__restrict__ step, const int *__restrict__ indices,
                                 int nsteps, const float2 *__restrict__ weights, int nfreq,
                                 const float *__restrict__ stage, int T,
@@ -256,17 +260,18 @@ __global__ void dft_fold_kernel(const int *__restrict__ step, const int *__restr
         valid[j] = (j < n && t < nsteps && indices[t] >= 0) ? 1 : 0;
     }
     __syncthreads();
-    // one thread per (frequency, component, cell): the staged samples of a
-    // cell are read (from L2) by its frequencies' threads; each phasor sums its
-    // steps in time order
+    const int groups = (nfreq + FOLD_K - 1) / FOLD_K;
     const i64 gid = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (gid >= (i64)nfreq * 6 * count) return;
-    const int k = (int)(gid / (6 * count));
-    const i64 rem = gid - (i64)k * 6 * count;
+    if (gid >= (i64)groups * 6 * count) return;
+    const int kg = (int)(gid / (6 * count));
+    const i64 rem = gid - (i64)kg * 6 * count;
     const int c = (int)(rem / count);
     const i64 i = rem - (i64)c * count;
-    double2 *p = phasor + ((i64)k * 6 + c) * count + i;
-    double2 acc = *p;
+    const int k0 = kg * FOLD_K, kn = min(FOLD_K, nfreq - k0);
+    double2 acc[FOLD_K];
+#pragma unroll
+    for (int q = 0; q < FOLD_K; ++q)
+        if (q < kn) acc[q] = phasor[((i64)(k0 + q) * 6 + c) * count + i];
     constexpr int CH = 8;  // samples in flight per thread
     for (int d0 = 0; d0 < n; d0 += CH) {
         float v[CH];
@@ -279,15 +284,21 @@ __global__ void dft_fold_kernel(const int *__restrict__ step, const int *__restr
         for (int j = 0; j < CH; ++j) {
             const int dt = d0 + j;
             if (dt >= n || !valid[dt]) continue;
-            const float2 w = wsm[k * T + dt];
-            const double wr = w.x, wi = w.y;
-            if (wr == 0.0 && wi == 0.0) continue;
             const double vv = (double)v[j];
-            acc.x = acc.x + wr * vv;
-            acc.y = acc.y + wi * vv;
+#pragma unroll
+            for (int q = 0; q < FOLD_K; ++q) {
+                if (q >= kn) break;
+                const float2 w = wsm[(k0 + q) * T + dt];
+                const double wr = w.x, wi = w.y;
+                if (wr == 0.0 && wi == 0.0) continue;
+                acc[q].x = acc[q].x + wr * vv;
+                acc[q].y = acc[q].y + wi * vv;
+            }
         }
     }
-    *p = acc;
+#pragma unroll
+    for (int q = 0; q < FOLD_K; ++q)
+        if (q < kn) phasor[((i64)(k0 + q) * 6 + c) * count + i] = acc[q];
 }
 
 }  // namespace wfb
@@ -362,7 +373,7 @@ int fdtd_dft_fold(const int *step, const int *indices, int nsteps, const float *
         set_error("fdtd_dft_fold: invalid arguments");
         return FDTD_ERR_ARG;
     }
-    const i64 work = (i64)nfreq * 6 * count;
+    const i64 work = (i64)((nfreq + FOLD_K - 1) / FOLD_K) * 6 * count;
     const size_t smem = (size_t)nfreq * T * sizeof(float2);
     dft_fold_kernel<<<(unsigned)((work + 255) / 256), 256, smem, (cudaStream_t)stream>>>(
         step, indices, nsteps, (const float2 *)weights, nfreq, stage, T, (double2 *)phasor,
