@@ -9,13 +9,15 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 
-def test_reverse_halves_match_prepare_gather_bitwise():
+@pytest.mark.parametrize("nz", [16, 15])
+def test_reverse_halves_match_prepare_gather_bitwise(nz):
+    """Rows of whole 16-byte vectors and ragged rows."""
     from warp_fdtd_b200 import _lib
     from warp_fdtd_b200 import adjoint as k
     from warp_fdtd_b200._lib import ptr
 
     rng = np.random.default_rng(3)
-    nx, ny, nz = 21, 18, 16
+    nx, ny = 21, 18
     n = nx * ny * nz
     box = (4, 3, 5, 9, 7, 6)
     dn = box[3] * box[4] * box[5]
