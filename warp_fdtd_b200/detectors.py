@@ -157,19 +157,28 @@ class Monitor:
                 *self.shape, int(self.axis), int(self.exact), stream,
             )
 
-    def phasors(self, k=0):
+    def _accumulator(self):
         owner = self.shared or self
         acc = owner.phasor
         if owner.is_phasor and owner._folded < self._solver._issued:
             # mid-batch read: add the pending steps to a copy
             acc = owner.phasor.clone()
             owner.fold(self._solver, self._solver._issued, into=acc)
-        raw = acc[k].cpu().numpy()
+        return acc
+
+    def phasors(self, k=0):
+        raw = self._accumulator()[k].cpu().numpy()
         return (raw[..., 0] + 1j * raw[..., 1]).reshape(6, *self.shape)
 
-    def power(self, s, k=0):
-        """detectors.py:203-211 (complex128 overlap on the host)."""
-        ph = self.phasors(k)
+    def all_phasors(self):
+        """Every frequency's phasors, (K, 6, *shape) complex128, in one copy."""
+        raw = self._accumulator().cpu().numpy()
+        return (raw[..., 0] + 1j * raw[..., 1]).reshape(raw.shape[0], 6, *self.shape)
+
+    def power(self, s, k=0, ph=None):
+        """detectors.py:203-211 (complex128 overlap on the host); `ph` the
+        frequency's phasors when the caller already holds them."""
+        ph = self.phasors(k) if ph is None else ph
         me = s.data[self.name + "/_mode_E"]
         mh = s.data[self.name + "/_mode_H"]
         em = me[k if me.shape[0] > 1 else 0]
@@ -202,7 +211,14 @@ def measurements(solver, k=0):
     """detectors.py:223-232 at frequency index k; with K > 1 frequencies the
     per-frequency values are added as `<name>_spectrum` lists."""
     modal = [m for m in solver.monitors if m.obj["class"] == "ModeOverlapDetector"]
-    powers = {m.name: m.power(solver, k) for m in modal}
+    # one device-to-host copy per accumulator (monitors of one plane share it)
+    held = {}
+    for m in modal:
+        key = id(m.shared or m)
+        if key not in held:
+            held[key] = m.all_phasors()
+    ph = lambda m, j: held[id(m.shared or m)][j]  # noqa: E731
+    powers = {m.name: m.power(solver, k, ph(m, k)) for m in modal}
     if powers:
         powers["modal_transmission"] = powers["mode_out"] / powers["mode_in"]
         if "mode_reflected" in powers:
@@ -210,7 +226,7 @@ def measurements(solver, k=0):
         K = min(len(m.frequencies) for m in modal)
         if K > 1:
             for m in modal:
-                powers[m.name + "_spectrum"] = [m.power(solver, j) for j in range(K)]
+                powers[m.name + "_spectrum"] = [m.power(solver, j, ph(m, j)) for j in range(K)]
             powers["modal_transmission_spectrum"] = [
                 a / b for a, b in zip(powers["mode_out_spectrum"], powers["mode_in_spectrum"])
             ]
