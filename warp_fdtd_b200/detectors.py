@@ -171,9 +171,29 @@ class Monitor:
         return (raw[..., 0] + 1j * raw[..., 1]).reshape(6, *self.shape)
 
     def all_phasors(self):
-        """Every frequency's phasors, (K, 6, *shape) complex128, in one copy."""
-        raw = self._accumulator().cpu().numpy()
-        return (raw[..., 0] + 1j * raw[..., 1]).reshape(raw.shape[0], 6, *self.shape)
+        """Every frequency's phasors, (K, 6, *shape) complex128, in one copy
+        (the float64 (re, im) pairs read as complex numbers in place)."""
+        raw = np.ascontiguousarray(self._accumulator().cpu().numpy())
+        return raw.view(np.complex128)[..., 0].reshape(raw.shape[0], 6, *self.shape)
+
+    def powers(self, s, ph_all):
+        """power() at every frequency of `ph_all` (all_phasors()).  Only the
+        normal component of the two cross products is formed, with
+        np.cross's own products and order, so each value equals power()'s."""
+        me = s.data[self.name + "/_mode_E"]
+        mh = s.data[self.name + "/_mode_H"]
+        b, c = (self.axis + 1) % 3, (self.axis + 2) % 3
+        out = []
+        for k in range(ph_all.shape[0]):
+            ph = ph_all[k]
+            em = me[k if me.shape[0] > 1 else 0]
+            hm = mh[k if mh.shape[0] > 1 else 0]
+            hc = ph[3:].conj()
+            ec = ph[:3].conj()
+            integrand = (em[b] * hc[c] - em[c] * hc[b]) + (ec[b] * hm[c] - ec[c] * hm[b])
+            alpha = np.sum(integrand * self.area_numpy) / 4
+            out.append(float(abs(alpha) ** 2))
+        return out
 
     def power(self, s, k=0, ph=None):
         """detectors.py:203-211 (complex128 overlap on the host); `ph` the
@@ -212,13 +232,14 @@ def measurements(solver, k=0):
     per-frequency values are added as `<name>_spectrum` lists."""
     modal = [m for m in solver.monitors if m.obj["class"] == "ModeOverlapDetector"]
     # one device-to-host copy per accumulator (monitors of one plane share it)
-    held = {}
+    # and every frequency's power from it
+    held, spectra = {}, {}
     for m in modal:
         key = id(m.shared or m)
         if key not in held:
             held[key] = m.all_phasors()
-    ph = lambda m, j: held[id(m.shared or m)][j]  # noqa: E731
-    powers = {m.name: m.power(solver, k, ph(m, k)) for m in modal}
+        spectra[m.name] = m.powers(solver, held[key])
+    powers = {m.name: spectra[m.name][k] for m in modal}
     if powers:
         powers["modal_transmission"] = powers["mode_out"] / powers["mode_in"]
         if "mode_reflected" in powers:
@@ -226,7 +247,7 @@ def measurements(solver, k=0):
         K = min(len(m.frequencies) for m in modal)
         if K > 1:
             for m in modal:
-                powers[m.name + "_spectrum"] = [m.power(solver, j, ph(m, j)) for j in range(K)]
+                powers[m.name + "_spectrum"] = spectra[m.name][:K]
             powers["modal_transmission_spectrum"] = [
                 a / b for a, b in zip(powers["mode_out_spectrum"], powers["mode_in_spectrum"])
             ]
