@@ -3,7 +3,8 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One bench step is one complete forward trajectory of the bend workload
-(reset + 4000 fused Yee steps + the two 5-wavelength modal detectors), i.e.
+(reset + 4000 Yee steps, two per launch of the time-blocked kernel, + the
+5-wavelength modal detectors at the input and output planes), i.e.
 6.05e10 cell-updates.  The metric is Gcell-updates/s over the whole job.
 Under torchrun (N > 1) every rank runs its own independent replica of the
 workload on its GPU (the path does not shard; there is no collective in the
@@ -11,8 +12,9 @@ data path) and `value` is the sum over ranks of cell-updates divided by the
 maximum over ranks of the device time.
 
 Printed on rank 0: one JSON line with the contract's keys plus `roofline`
-(the fused step kernel against the measured HBM copy bandwidth, 49 algorithmic
-bytes per cell-update), `cpu_baseline` (the CPU oracle on this host's cores on
+(the time-blocked step kernel against the measured HBM copy bandwidth, 49
+algorithmic bytes per cell-update, two cell-updates per launch, and its DRAM
+traffic measured by ncu on this grid), `cpu_baseline` (the CPU oracle on this host's cores on
 a bounded sample of the same grid), `e2e` (the same metric through the public
 Solver API with the material grid uploaded from pinned host memory and the
 detector phasors read back every step), `clocks` and `gpu_launches`.
@@ -49,6 +51,26 @@ WORKLOADS = {
 WORKLOAD = "bend20nm_324x324x144_4000steps_5lambda"
 METRIC = "Gcell-updates/s (20 nm bend forward)"
 BYTES_PER_CELL = 49  # read E, H (24 B) + write E, H (24 B) + 1 B material index
+
+
+def workload_config(workload, shape, time_steps, world):
+    """The `config` object of both arms' JSON lines."""
+    cells = int(np.prod(shape))
+    return {"workload": WORKLOAD if workload == "bend20" and time_steps == 4000
+            else f"{workload}_{list(shape)}_{time_steps}steps",
+            "grid": list(shape), "time_steps": int(time_steps), "cells": cells,
+            "materials": "uint8 index (SiO2 2.085, Si 12.11)",
+            "detectors": "mode_in (read forward and backward), mode_out x 5 "
+                         "wavelengths (float64 DFT)",
+            "pulse": "Hann, 200 fs, 1.55 um",
+            "l2": f"inputs larger than L2 (fields 4 x {cells * 12 / 1e6:.0f} MB ping-pong)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU"}
+
+
+def workload_shape(workload, time_steps=None):
+    """Grid and step count of a bench workload (20 nm cells, 12-cell CPML)."""
+    interior, steps = WORKLOADS[workload]
+    return tuple(int(round(v * 1e-6 / 20e-9)) + 24 for v in interior), time_steps or steps
 
 
 def load_peaks():
@@ -251,8 +273,8 @@ def run_reference(args, world, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000 * statistics.median(secs), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "grid": [324, 324, 144], "time_steps": 4000,
-                   "l2": "inputs larger than L2"},
+        "config": workload_config(args.workload, *workload_shape(args.workload, args.time_steps),
+                                  world),
         "cpu_baseline": {"value": value, "unit": "Gcell-updates/s", "cores": cores,
                          "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0,
@@ -418,15 +440,7 @@ def run_ours(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD if args.workload == "bend20" and s.steps == 4000
-                       else f"{args.workload}_{list(s.shape)}_{s.steps}steps",
-                       "grid": list(s.shape), "time_steps": s.steps,
-                       "cells": s.n, "materials": "uint8 index (SiO2 2.085, Si 12.11)",
-                       "detectors": "mode_in (read forward and backward), mode_out x 5 "
-                                    "wavelengths (float64 DFT)",
-                       "pulse": "Hann, 200 fs, 1.55 um",
-                       "l2": "inputs larger than L2 (fields 4 x 181 MB ping-pong)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "config": workload_config(args.workload, s.shape, s.steps, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": kernel_name, "cell_updates_per_launch": updates,
