@@ -3,15 +3,18 @@
 Same constructor, validation (ValueError messages), attributes and methods as
 the reference `Solver` (solver.py:53-264).  What changes underneath:
 
-* one fused E+H kernel per step (csrc/step_fused.cu) instead of two sweeps;
-  fields and CPML state ping-pong between two buffers, so `E`, `H` and `hprev`
-  are views of the buffer the step counter's parity selects and no hprev copy
-  is ever written;
+* fused E+H kernels instead of two sweeps per step: on the slab-CPML path
+  (the default when rows fit one TMA box) the time-blocked kernel advances two
+  steps per launch inside run() (csrc/step_block.cu, `time_block`), else one
+  fused step per launch (csrc/step_fz.cu, step_tma.cu, step_fused.cu); fields
+  and CPML state ping-pong between two buffers, so `E`, `H` and `hprev` are
+  views of the buffer the step counter's parity selects and no hprev copy is
+  ever written;
 * materials are stored as uint8 indices into an inverse-permittivity table
   when the grid has at most 256 distinct values (material="auto"), else as
   float32 per cell;
 * detectors accumulate K-frequency DFTs in float64 (detectors.py);
-* graphs are torch CUDA graphs of `graph_steps` fused steps.
+* graphs are torch CUDA graphs of `graph_steps` steps.
 All device memory is torch tensors; every kernel runs through the C ABI.
 """
 
