@@ -447,6 +447,15 @@ int fdtd_record_stage_many(const float *E0, const float *E1, const float *H0, co
                            int *step, const fdtd_stage_plane *planes, int nplanes, int nx,
                            int ny, int nz, int pitch_z, unsigned *advance_counter, int delta,
                            void *stream);
+/* Two consecutive steps' staging in one launch (the time-blocked step's
+ * pair): fields[0..3] = (E0, E1, H0, H1) as fdtd_record_stage_many takes them
+ * for step t = step[0], fields[4..7] for step t + 1; step[0] advances by 2
+ * after every block has read it (advance_counter required).  The caller folds
+ * no plane between the two steps: every plane's T is even and the pair starts
+ * on an even step.  No reference counterpart. */
+int fdtd_record_stage_pair(const float *const *fields, int *step, const fdtd_stage_plane *planes,
+                           int nplanes, int nx, int ny, int nz, int pitch_z,
+                           unsigned *advance_counter, void *stream);
 
 /* Fold the steps staged since the last fold into the phasors, in time order:
  * run after fdtd_advance once every T steps and after the last step.  With

@@ -156,3 +156,26 @@ def test_inject_many_and_block_step_reject_bad_arguments(lib):
     assert L.fdtd_step_block(ctypes.byref(a), None, None, None) == -1
     plan.depth = 2
     assert L.fdtd_step_block(ctypes.byref(a), ctypes.byref(plan), None, None) == -1
+
+
+def test_pair_staging_rejects_bad_arguments(lib):
+    """fdtd_record_stage_pair checks its fields, planes and counter on the
+    host, before any launch (odd T would let a fold fall inside the pair)."""
+    from warp_fdtd_b200 import _lib
+
+    L = _lib.load()
+    fields = (ctypes.c_void_p * 8)(*([16] * 8))
+    planes = (_lib.StagePlane * 1)()
+    pl = planes[0]
+    pl.indices, pl.stage, pl.nsteps, pl.T = 16, 32, 10, 4
+    pl.sx, pl.sy, pl.sz = 1, 4, 4
+    step, counter = 64, 80
+    call = lambda f, n, c: L.fdtd_record_stage_pair(f, step, planes, n, 4, 4, 4, 4, c, None)  # noqa
+    assert call(fields, 0, counter) == -1  # no plane
+    assert call(fields, 9, counter) == -1  # more than eight
+    assert call(fields, 1, None) == -1  # no completion counter
+    fields[5] = None
+    assert call(fields, 1, counter) == -1 and b"null field pointer 5" in L.fdtd_last_error()
+    fields[5] = 16
+    pl.T = 1
+    assert call(fields, 1, counter) == -1 and b"T >= 2" in L.fdtd_last_error()

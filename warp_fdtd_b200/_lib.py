@@ -131,6 +131,7 @@ _SIGNATURES = {
     "fdtd_batch_release": [ctypes.POINTER(BatchPlan)],
     "fdtd_record_stage_many": [_p, _p, _p, _p, _p, ctypes.POINTER(StagePlane), _i, _i, _i, _i,
                                _i, _p, _i, _p],
+    "fdtd_record_stage_pair": [_p, _p, ctypes.POINTER(StagePlane), _i, _i, _i, _i, _i, _p, _p],
     "fdtd_record_volume": [_p, _p, _p, _p, _p, _p, _ll, _p, _i, _i, _p, _i, _i, _i, _i, _p],
     "fdtd_record": [_p, _p, _p, _ll, _p, _p, _p, _p, _p, _p, _i, _i, _i, _i, _i, _i, _i, _i,
                     _i, _i, _i, _i, _p],

@@ -196,7 +196,7 @@ __device__ __forceinline__ void stage_block_done(int *step, unsigned *done, int 
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        const unsigned blocks = gridDim.x * gridDim.y;
+        const unsigned blocks = gridDim.x * gridDim.y * gridDim.z;
         if (atomicAdd(done, 1u) == blocks - 1) {
             step[0] += delta;
             *done = 0;
@@ -205,14 +205,22 @@ __device__ __forceinline__ void stage_block_done(int *step, unsigned *done, int 
     }
 }
 
-__global__ void record_stage_many_kernel(const float *__restrict__ E0, const float *__restrict__ E1,
-                                         const float *__restrict__ H0, const float *__restrict__ H1,
-                                         int *step, const StagePlanes planes, int nx, int ny,
-                                         int nz, int pitch, unsigned *done, int delta) {
+// Field pointers of the steps one launch stages: blockIdx.z selects the step
+// (t + blockIdx.z) and its pointer set.
+struct StageFields {
+    const float *E0[2], *E1[2], *H0[2], *H1[2];
+};
+
+__global__ void record_stage_many_kernel(const StageFields f, int *step, const StagePlanes planes,
+                                         int nx, int ny, int nz, int pitch, unsigned *done,
+                                         int delta) {
     const fdtd_stage_plane &pl = planes.p[blockIdx.y];
     const i64 count = (i64)pl.sx * pl.sy * pl.sz;
     const i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    const int t = *(volatile int *)step;
+    const int z = blockIdx.z;
+    const float *__restrict__ E0 = f.E0[z], *__restrict__ E1 = f.E1[z];
+    const float *__restrict__ H0 = f.H0[z], *__restrict__ H1 = f.H1[z];
+    const int t = *(volatile int *)step + z;
     if (i < count && t >= 0 && t < pl.nsteps && pl.indices[t] >= 0) {
         const int s = t & 1;
         const float *e = s ? E0 : E1;
@@ -421,10 +429,56 @@ int fdtd_record_stage_many(const float *E0, const float *E1, const float *H0, co
         sp.p[j] = pl;
         most = count > most ? count : most;
     }
+    StageFields f;
+    f.E0[0] = f.E0[1] = E0;
+    f.E1[0] = f.E1[1] = E1;
+    f.H0[0] = f.H0[1] = H0;
+    f.H1[0] = f.H1[1] = H1;
     record_stage_many_kernel<<<dim3((unsigned)((most + 255) / 256), (unsigned)nplanes), 256, 0,
-                               (cudaStream_t)stream>>>(E0, E1, H0, H1, step, sp, nx, ny, nz, pitch_z,
+                               (cudaStream_t)stream>>>(f, step, sp, nx, ny, nz, pitch_z,
                                                        advance_counter, delta);
     return launch_status("fdtd_record_stage_many");
+}
+
+int fdtd_record_stage_pair(const float *const *fields, int *step, const fdtd_stage_plane *planes,
+                           int nplanes, int nx, int ny, int nz, int pitch_z,
+                           unsigned *advance_counter, void *stream) {
+    if (pitch_z <= 0) pitch_z = nz;
+    if (!fields || !planes || nplanes < 1 || nplanes > FDTD_STAGE_PLANES_MAX || !step ||
+        !advance_counter || pitch_z < nz) {
+        set_error("fdtd_record_stage_pair: invalid arguments");
+        return FDTD_ERR_ARG;
+    }
+    for (int j = 0; j < 8; ++j)
+        if (!fields[j]) {
+            set_error("fdtd_record_stage_pair: null field pointer %d", j);
+            return FDTD_ERR_ARG;
+        }
+    StagePlanes sp;
+    i64 most = 0;
+    for (int j = 0; j < nplanes; ++j) {
+        const fdtd_stage_plane &pl = planes[j];
+        const i64 count = (i64)pl.sx * pl.sy * pl.sz;
+        if (count <= 0 || pl.T < 2 || pl.T > 256 || pl.nsteps < 1 || !pl.indices || !pl.stage ||
+            pl.x0 < 0 || pl.y0 < 0 || pl.z0 < 0 || pl.x0 + pl.sx > nx || pl.y0 + pl.sy > ny ||
+            pl.z0 + pl.sz > nz) {
+            set_error("fdtd_record_stage_pair: invalid plane %d (T >= 2 needed)", j);
+            return FDTD_ERR_ARG;
+        }
+        sp.p[j] = pl;
+        most = count > most ? count : most;
+    }
+    StageFields f;
+    for (int k = 0; k < 2; ++k) {
+        f.E0[k] = fields[4 * k];
+        f.E1[k] = fields[4 * k + 1];
+        f.H0[k] = fields[4 * k + 2];
+        f.H1[k] = fields[4 * k + 3];
+    }
+    record_stage_many_kernel<<<dim3((unsigned)((most + 255) / 256), (unsigned)nplanes, 2), 256, 0,
+                               (cudaStream_t)stream>>>(f, step, sp, nx, ny, nz, pitch_z,
+                                                       advance_counter, 2);
+    return launch_status("fdtd_record_stage_pair");
 }
 
 }  // extern "C"

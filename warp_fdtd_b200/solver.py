@@ -729,6 +729,11 @@ class Solver:
         else:
             _lib.call("fdtd_advance", ptr(self.step), 1, stream)
         self._issued += 1
+        self._folds()
+
+    def _folds(self):
+        """Fold the staged steps of every phasor monitor whose batch ends at
+        the step just issued (or at the last step)."""
         for monitor in self.monitors:
             if monitor.is_phasor and (self._issued % monitor.batch == 0
                                       or self._issued == self.steps):
@@ -757,12 +762,42 @@ class Solver:
         midH = ptr(self._mid[1]) if self._mid is not None else ptr(self._H[cur ^ 1])
         # step t (parity s) samples E[s^1], H[s^1] and H(n-1/2) = H[s]; step
         # t+1 (parity s^1) samples E[s], H[s] and H(n+1/2) = H[s^1]
+        sets = []
         for src in (cur, cur ^ 1):
             E, H = [None, None], [None, None]
             E[s], E[s ^ 1] = ptr(self._E[src]), midE
             H[s], H[s ^ 1] = ptr(self._H[src]), midH
-            self._record(E, H, stream)
+            sets.append((E, H))
+        if self._pair_staging():
+            # both steps' planes staged by one launch, which also advances the
+            # counter by two; no fold falls between the two steps
+            planes, _ = self._staged_planes()
+            nx, ny, nz = self.shape
+            fields = (ctypes.c_void_p * 8)(*(sets[0][0] + sets[0][1] + sets[1][0] + sets[1][1]))
+            _lib.call("fdtd_record_stage_pair", fields, ptr(self.step), planes, len(planes),
+                      nx, ny, nz, self._pitch, ptr(self._advance_counter), stream)
+            for _ in range(2):
+                self._issued += 1
+                self._folds()
+        else:
+            for E, H in sets:
+                self._record(E, H, stream)
         self._rel ^= 1
+
+    def _pair_staging(self):
+        """Whether a pair's detectors can run as one staging launch: every
+        monitor records through the grouped staging (or shares a plane that
+        does), and no plane folds between the pair's two steps."""
+        planes, grouped = self._staged_planes()
+        if planes is None:
+            return False
+        mid = self._issued + 1
+        for m in self.monitors:
+            if getattr(m, "shared", None) is not None:
+                continue
+            if id(m) not in grouped or m.batch % 2 or mid % m.batch == 0 or mid == self.steps:
+                return False
+        return True
 
     def _segment(self, length, final):
         """Issue `length` steps: pairs where the time-blocked kernel runs them,
